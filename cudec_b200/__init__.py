@@ -1,0 +1,103 @@
+"""cudec_b200 — B200-native batch decompression behind the iderex/cudec C ABI.
+
+The product is the shared library `libcudec_b200.so` (C ABI in
+include/cudec.h). This module is the Python mirror of that ABI over ctypes:
+the same entry-point names, argument meaning and status values, used by the
+tests and the benchmark. Loading fails loudly if the library has not been
+built; nothing here decodes on the CPU.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcudec_b200.so")
+
+# cudec_status (include/cudec.h)
+OK = 0
+ERR_INVALID_ARGUMENT = 1
+ERR_CORRUPT_INPUT = 2
+ERR_OUTPUT_TOO_SMALL = 3
+ERR_CUDA = 4
+ERR_NOT_IMPLEMENTED = 5
+ERR_UNSUPPORTED = 6
+
+STATUS_NAMES = {
+    OK: "CUDEC_OK",
+    ERR_INVALID_ARGUMENT: "CUDEC_ERR_INVALID_ARGUMENT",
+    ERR_CORRUPT_INPUT: "CUDEC_ERR_CORRUPT_INPUT",
+    ERR_OUTPUT_TOO_SMALL: "CUDEC_ERR_OUTPUT_TOO_SMALL",
+    ERR_CUDA: "CUDEC_ERR_CUDA",
+    ERR_NOT_IMPLEMENTED: "CUDEC_ERR_NOT_IMPLEMENTED",
+    ERR_UNSUPPORTED: "CUDEC_ERR_UNSUPPORTED",
+}
+
+# cudec_mem_space
+MEM_HOST = 0
+MEM_DEVICE = 1
+
+
+class ChunkResult(ctypes.Structure):
+    """cudec_chunk_result: the fixed 16-byte per-chunk record."""
+    _fields_ = [("status", ctypes.c_int32), ("reserved", ctypes.c_uint32),
+                ("bytes_written", ctypes.c_uint64)]
+
+
+assert ctypes.sizeof(ChunkResult) == 16
+
+_P = ctypes.c_void_p
+_SZ = ctypes.c_size_t
+
+# name -> (restype, argtypes); every symbol include/cudec.h declares.
+SIGNATURES = {
+    "cudec_version": (ctypes.c_int, []),
+    "cudec_lz4_decompress_batch": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P]),
+    "cudec_snappy_decompress_batch": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P]),
+}
+
+_lib = None
+
+
+def lib():
+    """The loaded decode library (built in-tree; raises if missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                "libcudec_b200.so is not built: run `python -m cudec_b200.build`")
+        handle = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_LOCAL)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def version():
+    return lib().cudec_version()
+
+
+def _batch_call(name, d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_caps, n,
+                d_results, stream):
+    return getattr(lib(), name)(d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_caps,
+                                n, d_results, stream)
+
+
+def lz4_decompress_batch(d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_caps, n,
+                         d_results, stream=None):
+    """cudec_lz4_decompress_batch: all pointers are device addresses (ints)."""
+    return _batch_call("cudec_lz4_decompress_batch", d_src_ptrs, d_src_sizes,
+                       d_dst_ptrs, d_dst_caps, n, d_results, stream)
+
+
+def snappy_decompress_batch(d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_caps, n,
+                            d_results, stream=None):
+    """cudec_snappy_decompress_batch (same contract as the LZ4 entry)."""
+    return _batch_call("cudec_snappy_decompress_batch", d_src_ptrs, d_src_sizes,
+                       d_dst_ptrs, d_dst_caps, n, d_results, stream)
+
+
+BATCH_ENTRIES = {
+    "lz4": lz4_decompress_batch,
+    "snappy": snappy_decompress_batch,
+}

@@ -1,0 +1,114 @@
+// C-ABI batch entries for the byte-oriented LZ formats (LZ4, raw Snappy).
+//
+// Contract (include/cudec.h): synchronous validation with no CUDA call on a
+// reject, then the pending CUDA error is consumed, the kernel is submitted on
+// the caller's stream, and the submission status is returned. Replaces
+// iderex/cudec src/batch.cu:6-31 with validate_batch_args at
+// src/lz4_decode.cuh:187-201 and the limit at src/batch_limits.h:28.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+
+#include "cudec.h"
+#include "launch.h"
+#include "lz_block_kernel.cuh"
+
+namespace cdb {
+
+cudec_status validate_batch(const void* const* src, const size_t* src_sizes,
+                            void* const* dst, const size_t* caps, size_t n,
+                            const cudec_chunk_result* results) {
+    if (src == nullptr || src_sizes == nullptr || dst == nullptr ||
+        caps == nullptr || results == nullptr ||
+        reinterpret_cast<uintptr_t>(results) % 16 != 0 || n == 0 ||
+        n > kMaxBatchChunks) {
+        return CUDEC_ERR_INVALID_ARGUMENT;
+    }
+    return CUDEC_OK;
+}
+
+namespace {
+
+// Per-device one-time setup: the kernels need more than 48 KB of dynamic
+// shared memory, which must be opted into once per device and kernel.
+constexpr int kMaxDevices = 64;
+std::atomic<int> g_lz4_ready[kMaxDevices];
+std::atomic<int> g_snappy_ready[kMaxDevices];
+std::atomic<int> g_sm_count[kMaxDevices];
+
+template <class Fmt>
+cudaError_t prepare(std::atomic<int>* ready, int dev) {
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    if (ready[dev].load(std::memory_order_acquire)) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(lz_decode_kernel<Fmt>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(kLzSmemBytes));
+    if (e != cudaSuccess) return e;
+    ready[dev].store(1, std::memory_order_release);
+    return cudaSuccess;
+}
+
+}  // namespace
+
+int device_sm_count(int dev) {
+    if (dev < 0 || dev >= kMaxDevices) return 0;
+    int v = g_sm_count[dev].load(std::memory_order_relaxed);
+    if (v > 0) return v;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+        return 0;
+    g_sm_count[dev].store(v, std::memory_order_relaxed);
+    return v;
+}
+
+template <class Fmt>
+static cudec_status launch_lz(std::atomic<int>* ready, const void* const* src,
+                              const size_t* src_sizes, void* const* dst,
+                              const size_t* caps, size_t n,
+                              cudec_chunk_result* results,
+                              cudaStream_t stream) {
+    const cudec_status v = validate_batch(src, src_sizes, dst, caps, n, results);
+    if (v != CUDEC_OK) return v;
+    (void)cudaGetLastError();
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return CUDEC_ERR_CUDA;
+    if (prepare<Fmt>(ready, dev) != cudaSuccess) return CUDEC_ERR_CUDA;
+    const int sms = device_sm_count(dev);
+    if (sms <= 0) return CUDEC_ERR_CUDA;
+    const size_t max_blocks = static_cast<size_t>(sms) * 2;
+    const unsigned grid = static_cast<unsigned>(n < max_blocks ? n : max_blocks);
+    lz_decode_kernel<Fmt><<<grid, kThreads, kLzSmemBytes, stream>>>(
+        src, src_sizes, dst, caps, n, results);
+    return cudaGetLastError() == cudaSuccess ? CUDEC_OK : CUDEC_ERR_CUDA;
+}
+
+}  // namespace cdb
+
+extern "C" {
+
+cudec_status cudec_lz4_decompress_batch(const void* const* d_src_ptrs,
+                                        const size_t* d_src_sizes,
+                                        void* const* d_dst_ptrs,
+                                        const size_t* d_dst_capacities,
+                                        size_t chunk_count,
+                                        cudec_chunk_result* d_results,
+                                        cudec_stream_t stream) {
+    return cdb::launch_lz<cdb::Lz4Format>(
+        cdb::g_lz4_ready, d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_capacities,
+        chunk_count, d_results, reinterpret_cast<cudaStream_t>(stream));
+}
+
+cudec_status cudec_snappy_decompress_batch(const void* const* d_src_ptrs,
+                                           const size_t* d_src_sizes,
+                                           void* const* d_dst_ptrs,
+                                           const size_t* d_dst_capacities,
+                                           size_t chunk_count,
+                                           cudec_chunk_result* d_results,
+                                           cudec_stream_t stream) {
+    return cdb::launch_lz<cdb::SnappyFormat>(
+        cdb::g_snappy_ready, d_src_ptrs, d_src_sizes, d_dst_ptrs,
+        d_dst_capacities, chunk_count, d_results,
+        reinterpret_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

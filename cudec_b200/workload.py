@@ -1,0 +1,141 @@
+"""Synthetic workloads with the benchmark configurations' shapes.
+
+Content comes from libcudec_workload.so (seeded SplitMix64 generator, see
+csrc/workload.c); compression uses the codec libraries the reference pins —
+liblz4's LZ4_compress_default (reached through ctypes, as the reference's
+fixtures reach it) and snappy's raw-block compressor (bundled in pyarrow;
+no libsnappy is installed on these hosts).
+
+The reference measures on Silesia/enwik8, which are not available; these
+seeded generators stand in for them with the distributions the benchmark
+configurations name.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+WORKLOAD_LIB = os.path.join(HERE, "libcudec_workload.so")
+
+
+class GenParams(ctypes.Structure):
+    _fields_ = [("copy_prob", ctypes.c_double), ("alphabet", ctypes.c_int),
+                ("zipf_s", ctypes.c_double), ("mean_lit", ctypes.c_double),
+                ("mean_match", ctypes.c_double), ("min_match", ctypes.c_uint32),
+                ("max_match", ctypes.c_uint32), ("max_offset", ctypes.c_uint64),
+                ("rle_prob", ctypes.c_double), ("mean_rle", ctypes.c_double),
+                ("random_bytes", ctypes.c_int)]
+
+
+def lz_params(copy_prob=0.5, random_bytes=False):
+    """LZ4/Snappy content: 64-symbol Zipf(1.1) literals (mean run 8), copies of
+    length 4-255 (geometric mean 16) at offsets uniform in 1..min(pos, 65535)."""
+    return GenParams(copy_prob, 64, 1.1, 8.0, 16.0, 4, 255, 65535, 0.0, 1.0,
+                     1 if random_bytes else 0)
+
+
+_wl = None
+_lz4 = None
+
+
+def _wlib():
+    global _wl
+    if _wl is None:
+        if not os.path.exists(WORKLOAD_LIB):
+            raise RuntimeError("libcudec_workload.so is not built: run "
+                               "`python -m cudec_b200.build`")
+        _wl = ctypes.CDLL(WORKLOAD_LIB)
+        _wl.gen_chunk.argtypes = [ctypes.c_uint64, ctypes.c_void_p,
+                                  ctypes.c_uint64, ctypes.POINTER(GenParams)]
+        _wl.gen_batch.argtypes = [ctypes.c_void_p, ctypes.c_void_p,
+                                  ctypes.c_void_p, ctypes.c_void_p,
+                                  ctypes.POINTER(GenParams), ctypes.c_void_p,
+                                  ctypes.c_uint64, ctypes.c_int]
+    return _wl
+
+
+def chunk_seed(base_seed, config_id, index):
+    return (base_seed ^ (config_id << 32) ^ index) & 0xFFFFFFFFFFFFFFFF
+
+
+def generate(sizes, params, param_idx=None, seeds=None, threads=None):
+    """Generate len(sizes) chunks into one contiguous uint8 buffer.
+    Returns (buffer, offsets)."""
+    sizes = np.asarray(sizes, dtype=np.uint64)
+    n = len(sizes)
+    offsets = np.zeros(n, dtype=np.uint64)
+    if n > 1:
+        offsets[1:] = np.cumsum(sizes[:-1])
+    buf = np.empty(int(sizes.sum()) if n else 0, dtype=np.uint8)
+    if seeds is None:
+        seeds = np.arange(n, dtype=np.uint64)
+    seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
+    if isinstance(params, GenParams):
+        params = [params]
+    parr = (GenParams * len(params))(*params)
+    if param_idx is None:
+        param_idx = np.zeros(n, dtype=np.int32)
+    param_idx = np.ascontiguousarray(param_idx, dtype=np.int32)
+    threads = threads or os.cpu_count() or 1
+    _wlib().gen_batch(seeds.ctypes.data, buf.ctypes.data, offsets.ctypes.data,
+                      sizes.ctypes.data, parr, param_idx.ctypes.data, n, threads)
+    return buf, offsets
+
+
+def _lz4lib():
+    global _lz4
+    if _lz4 is None:
+        _lz4 = ctypes.CDLL("liblz4.so.1")
+        _lz4.LZ4_compress_default.argtypes = [ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_int, ctypes.c_int]
+        _lz4.LZ4_compressBound.argtypes = [ctypes.c_int]
+        _lz4.LZ4_decompress_safe.argtypes = [ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_int, ctypes.c_int]
+    return _lz4
+
+
+def lz4_version():
+    return _lz4lib().LZ4_versionNumber()
+
+
+def lz4_compress(data):
+    """One raw LZ4 block via liblz4 LZ4_compress_default."""
+    data = np.ascontiguousarray(np.frombuffer(bytes(data), dtype=np.uint8)
+                                if not isinstance(data, np.ndarray) else data)
+    L = _lz4lib()
+    bound = L.LZ4_compressBound(len(data))
+    out = np.empty(max(bound, 1), dtype=np.uint8)
+    n = L.LZ4_compress_default(data.ctypes.data, out.ctypes.data, len(data), bound)
+    if n <= 0 and len(data) > 0:
+        raise RuntimeError("LZ4_compress_default failed")
+    return out[:n].tobytes()
+
+
+def lz4_decompress_ref(comp, cap):
+    """liblz4 LZ4_decompress_safe: returns bytes or None when liblz4 rejects."""
+    if len(comp) == 0:
+        return None
+    src = np.frombuffer(comp, dtype=np.uint8)
+    out = np.empty(max(cap, 1), dtype=np.uint8)
+    n = _lz4lib().LZ4_decompress_safe(src.ctypes.data, out.ctypes.data,
+                                      len(comp), cap)
+    return None if n < 0 else out[:n].tobytes()
+
+
+def snappy_codec():
+    import pyarrow
+    return pyarrow.Codec("snappy")
+
+
+def snappy_compress(data):
+    return snappy_codec().compress(bytes(data), asbytes=True)
+
+
+def snappy_decompress_ref(comp, declared):
+    """snappy raw decode via pyarrow: bytes or None when snappy rejects."""
+    try:
+        return snappy_codec().decompress(comp, decompressed_size=declared,
+                                         asbytes=True)
+    except Exception:  # pyarrow raises on any malformed stream
+        return None

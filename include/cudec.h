@@ -1,0 +1,121 @@
+/* cudec-b200: batch decompression for NVIDIA B200 (sm_100a).
+ *
+ * Public C ABI. Binary-compatible with the iderex/cudec interface
+ * (include/cudec.h of that project): the same status values, the same
+ * 16-byte per-chunk result record, the same entry-point signatures and the
+ * same synchronous/asynchronous split. A caller built against that header
+ * links against this library unchanged. Entry points that the reference does
+ * not ship carry the same contract shape and say so where they are declared.
+ *
+ * Nothing here needs CUDA headers. No entry point throws or longjmps across
+ * this boundary, and no output is reported that was not fully validated.
+ */
+#ifndef CUDEC_H
+#define CUDEC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CUDEC_VERSION_MAJOR 0
+#define CUDEC_VERSION_MINOR 1
+#define CUDEC_VERSION_PATCH 0
+
+/* Runtime library version, major * 10000 + minor * 100 + patch.
+ * Replaces: src/version.c:3-6 (declared include/cudec.h:26). */
+int cudec_version(void);
+
+/* Replaces: include/cudec.h:28-43. Values are fixed by the ABI. */
+typedef enum cudec_status {
+    CUDEC_OK = 0,
+    CUDEC_ERR_INVALID_ARGUMENT = 1,
+    CUDEC_ERR_CORRUPT_INPUT = 2,
+    CUDEC_ERR_OUTPUT_TOO_SMALL = 3,
+    CUDEC_ERR_CUDA = 4,
+    /* Kept at this value for exhaustive switches; no entry point returns it. */
+    CUDEC_ERR_NOT_IMPLEMENTED = 5,
+    /* Valid input outside the decoded subset (e.g. an LZ4 frame in
+     * block-linked mode, or one carrying a dictionary id). */
+    CUDEC_ERR_UNSUPPORTED = 6
+} cudec_status;
+
+/* Same representation as cudaStream_t (a pointer to CUstream_st). NULL is
+ * the legacy default stream. Replaces: include/cudec.h:49. */
+typedef struct CUstream_st* cudec_stream_t;
+
+/* Per-chunk outcome written by the device into caller memory.
+ * Replaces: include/cudec.h:53-78 (layout pinned below). */
+typedef struct cudec_chunk_result {
+    int32_t status;         /* a cudec_status value */
+    uint32_t reserved;      /* always written as zero */
+    uint64_t bytes_written; /* decoded bytes when status == CUDEC_OK, else 0 */
+} cudec_chunk_result;
+
+#if defined(__cplusplus) && __cplusplus >= 201103L
+static_assert(sizeof(cudec_chunk_result) == 16 &&
+                  offsetof(cudec_chunk_result, bytes_written) == 8,
+              "cudec_chunk_result is a fixed 16-byte record");
+#elif defined(__STDC_VERSION__) && __STDC_VERSION__ >= 201112L
+_Static_assert(sizeof(cudec_chunk_result) == 16 &&
+                   offsetof(cudec_chunk_result, bytes_written) == 8,
+               "cudec_chunk_result is a fixed 16-byte record");
+#else
+typedef char cudec_chunk_result_size_check
+    [(sizeof(cudec_chunk_result) == 16 &&
+      offsetof(cudec_chunk_result, bytes_written) == 8) ? 1 : -1];
+#endif
+
+/* ---------------------------------------------------------------------
+ * Batch block decode (device memory in, device memory out, asynchronous)
+ *
+ * Every array argument is a device array of chunk_count entries and every
+ * pointer held in them is a device pointer. d_results must be 16-byte
+ * aligned. Synchronous return: argument validation and launch submission
+ * only. Per-chunk outcomes land in d_results once `stream` reaches the end of
+ * the launch. A chunk that decodes reports CUDEC_OK and bytes_written, and
+ * exactly dst[0, bytes_written) was written. A chunk that does not reports
+ * CUDEC_ERR_CORRUPT_INPUT or CUDEC_ERR_OUTPUT_TOO_SMALL with bytes_written 0;
+ * its destination is then unspecified (never beyond its capacity).
+ *
+ * Validation failures return CUDEC_ERR_INVALID_ARGUMENT, launch nothing and
+ * make no CUDA call (the thread's pending CUDA error is left as it was): a
+ * NULL array, a misaligned d_results, chunk_count == 0, or chunk_count above
+ * the launch limit (2^31-1 warps of 32 chunks; rejected, never truncated).
+ * A call that passes validation consumes the pending CUDA error, so the
+ * returned status describes this submission alone. The library allocates
+ * nothing on this path. Thread-safe for distinct streams.
+ * ------------------------------------------------------------------- */
+
+/* LZ4 block format (one raw LZ4 block per chunk).
+ * Replaces: include/cudec.h:102-108, src/batch.cu:6-31. */
+cudec_status cudec_lz4_decompress_batch(const void* const* d_src_ptrs,
+                                        const size_t* d_src_sizes,
+                                        void* const* d_dst_ptrs,
+                                        const size_t* d_dst_capacities,
+                                        size_t chunk_count,
+                                        cudec_chunk_result* d_results,
+                                        cudec_stream_t stream);
+
+/* Raw Snappy block format (varint length preamble + elements; no framing).
+ * Not shipped by the reference: its design record commits this exact
+ * signature with "no deltas" from the LZ4 entry (docs/MASTERPLAN.md:720-740);
+ * the per-chunk rules follow src/snappy_block.h:58-436. The declared length
+ * above the chunk's capacity is CUDEC_ERR_OUTPUT_TOO_SMALL; every other
+ * inconsistency, including under- or over-production of the declared length,
+ * is CUDEC_ERR_CORRUPT_INPUT. */
+cudec_status cudec_snappy_decompress_batch(const void* const* d_src_ptrs,
+                                           const size_t* d_src_sizes,
+                                           void* const* d_dst_ptrs,
+                                           const size_t* d_dst_capacities,
+                                           size_t chunk_count,
+                                           cudec_chunk_result* d_results,
+                                           cudec_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUDEC_H */

@@ -1,0 +1,164 @@
+"""ORACLE — test infrastructure, not part of the product.
+
+ctypes loaders for:
+  liboracle.so          the C restatement of the reference ladders (oracle.c)
+                        and the multithreaded codec-library harness (codecs.c)
+  _ref/libref_twin.so   the reference's own host twins, compiled in place
+  _ref/libcudec_ref.so  the reference library (GPU), compiled in place
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use
+this package, and only as a checker or a timed baseline.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "liboracle.so")
+REF_TWIN_LIB = os.path.join(HERE, "_ref", "libref_twin.so")
+REF_GPU_LIB = os.path.join(HERE, "_ref", "libcudec_ref.so")
+
+_U8P = ctypes.c_void_p
+_U64 = ctypes.c_uint64
+_DEC = [_U8P, _U64, _U8P, _U64, ctypes.POINTER(_U64)]
+_BATCH = [_U8P, _U8P, _U8P, _U8P, _U64, _U8P, _U8P, ctypes.c_int]
+
+
+def build():
+    """Compile the restatement (and the reference pieces when its tree is
+    present) with oracle/Makefile."""
+    subprocess.run(["make", "-s", "-f", os.path.join(HERE, "Makefile")],
+                   check=True)
+
+
+_libs = {}
+
+
+def _load(path, funcs):
+    if path not in _libs:
+        if not os.path.exists(path):
+            return None
+        h = ctypes.CDLL(path, mode=ctypes.RTLD_LOCAL)
+        for name, (res, args) in funcs.items():
+            f = getattr(h, name)
+            f.restype = res
+            f.argtypes = args
+        _libs[path] = h
+    return _libs[path]
+
+
+def oracle_lib():
+    h = _load(ORACLE_LIB, {
+        "oracle_lz4_decode": (ctypes.c_int, _DEC),
+        "oracle_snappy_decode": (ctypes.c_int, _DEC),
+        "oracle_lz4_decode_batch": (ctypes.c_int, _BATCH),
+        "oracle_snappy_decode_batch": (ctypes.c_int, _BATCH),
+        "codec_decode_batch": (ctypes.c_int, [ctypes.c_int] + _BATCH),
+        "codec_lz4_version": (ctypes.c_int, []),
+        "codec_zstd_version": (ctypes.c_int, []),
+    })
+    if h is None:
+        raise RuntimeError("oracle/liboracle.so is not built (oracle.build())")
+    return h
+
+
+def ref_twin_lib():
+    """The reference's host twins, or None where they were not built."""
+    return _load(REF_TWIN_LIB, {
+        "ref_lz4_twin_decode": (ctypes.c_int, _DEC),
+        "ref_snappy_twin_decode": (ctypes.c_int, _DEC),
+        "ref_lz4_twin_decode_batch": (ctypes.c_int, _BATCH),
+        "ref_snappy_twin_decode_batch": (ctypes.c_int, _BATCH),
+    })
+
+
+def ref_gpu_lib():
+    """The reference library (sm_100a build), or None where it was not built."""
+    return _load(REF_GPU_LIB, {
+        "cudec_lz4_decompress_batch": (ctypes.c_int, [ctypes.c_void_p] * 4 +
+                                       [ctypes.c_size_t, ctypes.c_void_p,
+                                        ctypes.c_void_p]),
+        "cudec_version": (ctypes.c_int, []),
+    })
+
+
+def _decode_one(fn, comp, cap):
+    src = np.frombuffer(bytes(comp), dtype=np.uint8)
+    if len(src) == 0:
+        src = np.zeros(1, dtype=np.uint8)
+    out = np.zeros(max(cap, 1), dtype=np.uint8)
+    w = _U64(0)
+    st = fn(src.ctypes.data, len(comp), out.ctypes.data, cap, ctypes.byref(w))
+    return st, (out[:w.value].tobytes() if st == 0 else b"")
+
+
+def lz4_decode(comp, cap):
+    """(status, bytes) from the C restatement."""
+    return _decode_one(oracle_lib().oracle_lz4_decode, comp, cap)
+
+
+def snappy_decode(comp, cap):
+    return _decode_one(oracle_lib().oracle_snappy_decode, comp, cap)
+
+
+def ref_lz4_decode(comp, cap):
+    """(status, bytes) from the reference's own twin, or None if unbuilt."""
+    h = ref_twin_lib()
+    return None if h is None else _decode_one(h.ref_lz4_twin_decode, comp, cap)
+
+
+def ref_snappy_decode(comp, cap):
+    h = ref_twin_lib()
+    return None if h is None else _decode_one(h.ref_snappy_twin_decode, comp, cap)
+
+
+class HostBatch:
+    """Chunks packed in host memory with pointer/size tables, for the batch
+    drivers (restatement, reference twin, codec libraries)."""
+
+    def __init__(self, comps, caps):
+        self.n = len(comps)
+        sizes = np.array([len(c) for c in comps], dtype=np.uint64)
+        self.src = np.frombuffer(b"".join(comps) + b"\0", dtype=np.uint8).copy()
+        offs = np.zeros(self.n, dtype=np.uint64)
+        if self.n > 1:
+            offs[1:] = np.cumsum(sizes[:-1])
+        self.src_sizes = sizes
+        self.caps = np.asarray(caps, dtype=np.uint64)
+        dst_offs = np.zeros(self.n, dtype=np.uint64)
+        if self.n > 1:
+            dst_offs[1:] = np.cumsum(self.caps[:-1])
+        self.dst = np.zeros(int(self.caps.sum()) + 1, dtype=np.uint8)
+        self.src_ptrs = (offs + self.src.ctypes.data).astype(np.uint64)
+        self.dst_ptrs = (dst_offs + self.dst.ctypes.data).astype(np.uint64)
+        self.dst_offs = dst_offs
+        self.status = np.zeros(self.n, dtype=np.int32)
+        self.written = np.zeros(self.n, dtype=np.uint64)
+
+    def args(self):
+        return (self.src_ptrs.ctypes.data, self.src_sizes.ctypes.data,
+                self.dst_ptrs.ctypes.data, self.caps.ctypes.data, self.n,
+                self.status.ctypes.data, self.written.ctypes.data)
+
+    def output(self, i):
+        o = int(self.dst_offs[i])
+        return self.dst[o:o + int(self.written[i])].tobytes()
+
+
+def decode_batch(kind, batch, threads):
+    """Run a batch driver: kind in {"oracle_lz4", "oracle_snappy", "ref_lz4",
+    "ref_snappy", "codec_lz4", "codec_zstd"}. Returns the thread count used."""
+    if kind.startswith("oracle_"):
+        fn = getattr(oracle_lib(), "oracle_%s_decode_batch" % kind[7:])
+        return fn(*batch.args(), threads)
+    if kind.startswith("ref_"):
+        h = ref_twin_lib()
+        if h is None:
+            raise RuntimeError("reference twins not built")
+        return getattr(h, "ref_%s_twin_decode_batch" % kind[4:])(*batch.args(), threads)
+    if kind.startswith("codec_"):
+        code = {"codec_lz4": 0, "codec_zstd": 1}[kind]
+        return oracle_lib().codec_decode_batch(code, *batch.args(), threads)
+    raise ValueError(kind)

@@ -1,0 +1,96 @@
+"""ABI conformance without a GPU (the reference's tests/conformance_c.c:34-120
+checks, plus the exported-symbol set).
+
+Validation rejects make no CUDA call, so they run on a host with no device.
+"""
+import ctypes
+import os
+import re
+import subprocess
+
+import cudec_b200 as cd
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "cudec.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(cudec_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_exports_every_declared_symbol():
+    names = declared_functions()
+    assert "cudec_lz4_decompress_batch" in names
+    out = subprocess.run(["nm", "-D", "--defined-only", cd.LIB_PATH],
+                         capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r"\bT (cudec_[a-z0-9_]+)", out))
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+    # and the Python mirror binds each of them
+    assert set(names) <= set(cd.SIGNATURES), set(names) - set(cd.SIGNATURES)
+    lib = cd.lib()
+    for n in names:
+        assert getattr(lib, n) is not None
+
+
+def test_version_matches_header():
+    text = open(HEADER).read()
+    maj = int(re.search(r"CUDEC_VERSION_MAJOR (\d+)", text).group(1))
+    mnr = int(re.search(r"CUDEC_VERSION_MINOR (\d+)", text).group(1))
+    pat = int(re.search(r"CUDEC_VERSION_PATCH (\d+)", text).group(1))
+    assert cd.version() == maj * 10000 + mnr * 100 + pat
+
+
+def test_result_record_layout():
+    assert ctypes.sizeof(cd.ChunkResult) == 16
+    assert cd.ChunkResult.bytes_written.offset == 8
+
+
+def _fake(n=8):
+    # Non-NULL host addresses: validation must reject before touching them.
+    buf = (ctypes.c_uint8 * (64 * n + 64))()
+    base = ctypes.addressof(buf)
+    aligned = (base + 15) & ~15
+    return buf, aligned
+
+
+def test_batch_validation_rejects_synchronously():
+    buf, a = _fake()
+    for entry in cd.BATCH_ENTRIES.values():
+        ok_args = [a, a, a, a, 4, a]
+        for i in range(4):
+            args = list(ok_args)
+            args[i] = None
+            assert entry(*args, None) == cd.ERR_INVALID_ARGUMENT
+        assert entry(a, a, a, a, 4, None, None) == cd.ERR_INVALID_ARGUMENT
+        assert entry(a, a, a, a, 4, a + 8, None) == cd.ERR_INVALID_ARGUMENT
+        assert entry(a, a, a, a, 0, a, None) == cd.ERR_INVALID_ARGUMENT
+        assert entry(a, a, a, a, 2**64 - 1, a, None) == cd.ERR_INVALID_ARGUMENT
+        assert entry(a, a, a, a, (2**31 - 1) * 32 + 1, a, None) == cd.ERR_INVALID_ARGUMENT
+
+
+def test_c99_consumer_compiles_and_links(tmp_path):
+    """A plain C99 translation unit includes the header and links the library
+    (what tests/consumer and tests/conformance_c.c pin in the reference)."""
+    src = tmp_path / "consumer.c"
+    src.write_text(
+        '#include "cudec.h"\n#include <stdio.h>\n'
+        "int main(void) {\n"
+        "  cudec_chunk_result r; (void)r;\n"
+        "  if (cudec_version() != CUDEC_VERSION_MAJOR*10000 + CUDEC_VERSION_MINOR*100"
+        " + CUDEC_VERSION_PATCH) return 1;\n"
+        "  if (cudec_lz4_decompress_batch(NULL, NULL, NULL, NULL, 1, NULL, NULL)"
+        " != CUDEC_ERR_INVALID_ARGUMENT) return 2;\n"
+        "  if (cudec_snappy_decompress_batch(NULL, NULL, NULL, NULL, 1, NULL, NULL)"
+        " != CUDEC_ERR_INVALID_ARGUMENT) return 3;\n"
+        "  puts(\"ok\"); return 0;\n}\n")
+    exe = tmp_path / "consumer"
+    libdir = os.path.dirname(cd.LIB_PATH)
+    subprocess.run(["gcc", "-std=c99", "-pedantic", "-Wall", "-Werror", "-I",
+                    os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    "-L" + libdir, "-lcudec_b200", "-Wl,-rpath," + libdir],
+                   check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0 and out.stdout.strip() == "ok", (out.returncode, out.stderr)

@@ -1,0 +1,185 @@
+"""GPU parity for the LZ4 and Snappy batch entries (through the C ABI).
+
+Every chunk's status must equal the oracle's; a successful chunk's output is
+bit-exact and nothing past bytes_written is touched (destinations are
+poisoned with 0xA5 and results primed with 0xFF, as the reference's
+tests/gpu_fixture.cu:21,54 do). The reference's own GPU library (built from
+its sources into oracle/_ref) is run on the same LZ4 inputs where present.
+"""
+import ctypes
+import hashlib
+import json
+import os
+import random
+
+import numpy as np
+import pytest
+
+import oracle
+from cudec_b200 import workload as W
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+ORACLE = {"lz4": oracle.lz4_decode, "snappy": oracle.snappy_decode}
+COMPRESS = {"lz4": W.lz4_compress, "snappy": W.snappy_compress}
+
+
+def run_batch(cuda, fmt, comps, caps, **kw):
+    from cudec_b200.device import DeviceBatch
+    import torch
+    b = DeviceBatch(comps, caps, device=cuda, **kw)
+    assert b.run(fmt) == 0
+    torch.cuda.synchronize()
+    return b, b.results(), b.dst_host()
+
+
+def check_against_oracle(fmt, b, res, dst, comps, caps, label=""):
+    for i, (comp, cap) in enumerate(zip(comps, caps)):
+        st, out = ORACLE[fmt](comp, cap)
+        r = res[i]
+        assert r["status"] == st, (label, i, int(r["status"]), st, len(comp), cap)
+        assert r["reserved"] == 0
+        if st == 0:
+            assert r["bytes_written"] == len(out), (label, i)
+            got = b.output(i, dst, len(out))
+            assert got == out, (label, i, "bytes differ")
+            tail = b.output(i, dst)[len(out):]
+            assert tail == bytes([0xA5]) * len(tail), (label, i, "wrote past bytes_written")
+        else:
+            assert r["bytes_written"] == 0
+
+
+def gen(sizes, probs=None, randoms=(), seed=1):
+    n = len(sizes)
+    probs = probs or [0.5] * n
+    params = [W.lz_params(p, random_bytes=(i in randoms)) for i, p in enumerate(probs)]
+    buf, offs = W.generate(sizes, params, param_idx=np.arange(n),
+                           seeds=np.array([W.chunk_seed(seed, 0, i) for i in range(n)],
+                                          dtype=np.uint64))
+    return [buf[int(o):int(o) + int(s)].tobytes() for o, s in zip(offs, sizes)]
+
+
+@pytest.mark.parametrize("fmt,fixture", [("lz4", "lz4_block.json"),
+                                         ("snappy", "snappy_block.json")])
+def test_golden_vectors(cuda, fmt, fixture):
+    vecs = json.load(open(os.path.join(GOLDEN, fixture)))["vectors"]
+    comps = [bytes.fromhex(v["input_hex"]) for v in vecs]
+    caps = [v["capacity"] for v in vecs]
+    b, res, dst = run_batch(cuda, fmt, comps, caps)
+    for i, v in enumerate(vecs):
+        assert res[i]["status"] == v["expect_status"], v["name"]
+        if v["expect_status"] == 0:
+            out = b.output(i, dst, v["expect_len"])
+            assert hashlib.sha256(out).hexdigest() == v["expect_sha256"], v["name"]
+    check_against_oracle(fmt, b, res, dst, comps, caps, "golden")
+
+
+@pytest.mark.parametrize("fmt", ["lz4", "snappy"])
+def test_seeded_sizes_and_windows(cuda, fmt):
+    """Sizes from 1 B to 4 MiB: inputs spanning several 32 KiB staging windows,
+    outputs far past the 64 KiB shared ring, incompressible chunks (one long
+    literal run) and every copy probability."""
+    sizes = [1, 2, 5, 12, 13, 31, 64, 100, 1000, 4095, 4096, 4097, 65535, 65536,
+             65537, 100000, 262144, 1 << 20, 3 << 20, 4 << 20]
+    probs = [0.2 + 0.6 * (i % 7) / 6 for i in range(len(sizes))]
+    raws = gen(sizes, probs, randoms={3, 9, 16, 19}, seed=2)
+    comps = [COMPRESS[fmt](r) for r in raws]
+    caps = [len(r) for r in raws]
+    b, res, dst = run_batch(cuda, fmt, comps, caps)
+    check_against_oracle(fmt, b, res, dst, comps, caps, "sizes")
+    assert all(res["status"] == 0)
+
+
+@pytest.mark.parametrize("fmt", ["lz4", "snappy"])
+@pytest.mark.parametrize("skew", [(0, 0), (1, 3), (7, 15), (13, 1)])
+def test_unaligned_buffers(cuda, fmt, skew):
+    raws = gen([777, 65536, 70001, 200000], seed=3)
+    comps = [COMPRESS[fmt](r) for r in raws]
+    caps = [len(r) + 40 for r in raws]
+    b, res, dst = run_batch(cuda, fmt, comps, caps, dst_skew=skew[0], src_skew=skew[1])
+    check_against_oracle(fmt, b, res, dst, comps, caps, "skew")
+
+
+@pytest.mark.parametrize("fmt", ["lz4", "snappy"])
+def test_mutants_match_oracle(cuda, fmt):
+    rng = random.Random(9)
+    raws = gen([50, 3000, 40000, 70000], probs=[0.3, 0.5, 0.7, 0.5], seed=4)
+    comps, caps = [], []
+    for r in raws:
+        c = COMPRESS[fmt](r)
+        for k in range(40):
+            b = bytearray(c)
+            if k % 3 == 0:
+                b = b[:rng.randrange(max(len(b), 1))]
+            else:
+                for _ in range(rng.randint(1, 4)):
+                    if b:
+                        b[rng.randrange(len(b))] ^= 1 << rng.randrange(8)
+            comps.append(bytes(b))
+            caps.append(rng.choice([len(r), len(r) + 11, max(len(r) - 7, 0)]))
+    b, res, dst = run_batch(cuda, fmt, comps, caps)
+    check_against_oracle(fmt, b, res, dst, comps, caps, "mutants")
+
+
+@pytest.mark.parametrize("fmt", ["lz4", "snappy"])
+def test_overlapping_and_long_matches(cuda, fmt):
+    raws = [b"\x5a" * 65536, bytes((0, 255)) * 40000, b"abc" * 300000,
+            bytes(range(256)) * 4096, b"\x00" * (2 << 20)]
+    comps = [COMPRESS[fmt](r) for r in raws]
+    caps = [len(r) for r in raws]
+    b, res, dst = run_batch(cuda, fmt, comps, caps)
+    check_against_oracle(fmt, b, res, dst, comps, caps, "overlap")
+    assert all(res["status"] == 0)
+
+
+def test_config1_shape_bit_exact_and_deterministic(cuda):
+    """1,024 x 64 KiB LZ4 chunks (the headline workload), twice."""
+    raws = gen([65536] * 1024, seed=1234)
+    comps = [W.lz4_compress(r) for r in raws]
+    caps = [65536] * 1024
+    b, res, dst = run_batch(cuda, "lz4", comps, caps)
+    assert all(res["status"] == 0) and all(res["bytes_written"] == 65536)
+    for i in range(0, 1024, 37):
+        assert b.output(i, dst, 65536) == raws[i]
+    h1 = hashlib.sha256(dst.tobytes()).hexdigest()
+    b.reset()
+    import torch
+    assert b.run("lz4") == 0
+    torch.cuda.synchronize()
+    assert hashlib.sha256(b.dst_host().tobytes()).hexdigest() == h1
+    full = b.dst_host()
+    assert all(b.output(i, full, 65536) == raws[i] for i in range(1024))
+
+
+@pytest.mark.skipif(oracle.ref_gpu_lib() is None, reason="reference library not built")
+def test_matches_reference_gpu_library(cuda):
+    """Same inputs through the reference's own cudec_lz4_decompress_batch
+    (compiled for sm_100a from its sources): identical records and bytes."""
+    import torch
+    rng = random.Random(12)
+    raws = gen([100, 5000, 65536, 65536, 300000], seed=5)
+    comps, caps = [], []
+    for r in raws:
+        c = W.lz4_compress(r)
+        comps.append(c)
+        caps.append(len(r))
+        for _ in range(8):
+            m = bytearray(c)
+            m[rng.randrange(len(m))] ^= 1 << rng.randrange(8)
+            comps.append(bytes(m))
+            caps.append(len(r))
+    b, res, dst = run_batch(cuda, "lz4", comps, caps)
+    ref = oracle.ref_gpu_lib()
+    b.reset()
+    st = ref.cudec_lz4_decompress_batch(*[ctypes.c_void_p(a) for a in b.args()[:4]],
+                                        b.n, ctypes.c_void_p(b.args()[5]), None)
+    assert st == 0
+    torch.cuda.synchronize()
+    rres, rdst = b.results(), b.dst_host()
+    assert (rres["status"] == res["status"]).all()
+    assert (rres["bytes_written"] == res["bytes_written"]).all()
+    for i in range(b.n):
+        if res[i]["status"] == 0:
+            n = int(res[i]["bytes_written"])
+            assert b.output(i, dst, n) == b.output(i, rdst, n)
