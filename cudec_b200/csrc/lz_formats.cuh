@@ -41,6 +41,10 @@ struct InView {
 struct Seq {
     uint64_t lit_src, lit_len, match_len;
     uint32_t off;
+    // Every check that does not depend on the output position passed (and,
+    // for LZ4, the run is not a terminal one): `fast_ok` can then decide the
+    // sequence from its output position alone.
+    bool clean;
 };
 
 // --------------------------------------------------------------------------
@@ -94,12 +98,15 @@ struct Lz4Format {
         uint64_t lit = tok >> 4;
         s->match_len = 0;
         s->off = 1;
+        s->clean = false;
         if (lit == 15) {
+            if (q + 15 >= S) { s->lit_src = q; s->lit_len = 0; return; }
             uint32_t b;
             do {
                 if (q >= S) { s->lit_src = q; s->lit_len = 0; return; }
                 b = in.at(q++);
                 lit += b;
+                if (q + 15 > S) { s->lit_src = q; s->lit_len = 0; return; }
             } while (b == 255);
         }
         s->lit_src = q;
@@ -110,15 +117,26 @@ struct Lz4Format {
         s->off = in.at(q) | (in.at(q + 1) << 8);
         q += 2;
         uint64_t ml = (tok & 15) + 4;
+        bool ok = s->off != 0;
         if ((tok & 15) == 15) {
             uint32_t b;
             do {
-                if (q >= S) break;
+                if (q >= S) { ok = false; break; }
                 b = in.at(q++);
                 ml += b;
+                if (q + 4 > S) { ok = false; break; }
             } while (b == 255);
         }
         s->match_len = ml;
+        s->clean = ok;
+    }
+
+    // A clean, non-terminal sequence that fits with the end-of-block slack to
+    // spare passes every rung of `check` and is not the terminal run.
+    __device__ __forceinline__ static bool fast_ok(const Seq& s, uint64_t cap,
+                                                   uint64_t d) {
+        return s.clean && d <= cap && s.off <= d + s.lit_len &&
+               cap - d >= s.lit_len + s.match_len + kEndSlackDst;
     }
 
     // AccumulateLength (lz4_block.h:95-128): `room` = capacity - dst_pos.
@@ -238,6 +256,7 @@ struct SnappyFormat {
         s->match_len = 0;
         s->off = 1;
         s->lit_src = p;
+        s->clean = false;
         if (kind == 0) {
             const uint32_t l6 = tag >> 2;
             uint64_t hdr = 1, len = l6;
@@ -251,6 +270,7 @@ struct SnappyFormat {
             }
             s->lit_src = p + hdr;
             s->lit_len = len + 1;
+            s->clean = s->lit_len <= S - s->lit_src;
             return;
         }
         const uint32_t ob = kind == 1 ? 1 : (kind == 2 ? 2 : 4);
@@ -265,6 +285,16 @@ struct SnappyFormat {
             s->match_len = (tag >> 2) + 1;
         }
         s->off = static_cast<uint32_t>(off);
+        s->clean = off != 0;
+    }
+
+    // A clean element whose source and length fit the produced/declared
+    // bounds passes every rung of `check`.
+    __device__ __forceinline__ static bool fast_ok(const Seq& s, uint64_t declared,
+                                                   uint64_t d) {
+        const uint64_t len = s.lit_len + s.match_len;
+        return s.clean && d <= declared && len <= declared - d &&
+               (s.match_len == 0 || s.off <= d);
     }
 
     // `declared` is the preamble's length (already bounded by capacity).

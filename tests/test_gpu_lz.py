@@ -102,6 +102,20 @@ def test_unaligned_buffers(cuda, fmt, skew):
 
 
 @pytest.mark.parametrize("fmt", ["lz4", "snappy"])
+def test_short_periods_at_every_alignment(cuda, fmt):
+    """Matches whose period is shorter than a 16-byte vector, starting in the
+    first vectors of the destination, for every destination misalignment."""
+    raws = [b"ab" * 5000, b"x" + b"abc" * 7000, b"0123456789abcde" * 900,
+            b"q" * 3 + b"\x00\x01" * 9000, bytes(range(7)) * 3000]
+    comps = [COMPRESS[fmt](r) for r in raws]
+    caps = [len(r) for r in raws]
+    for skew in range(16):
+        b, res, dst = run_batch(cuda, fmt, comps, caps, dst_skew=skew, src_skew=(skew * 7) % 16)
+        check_against_oracle(fmt, b, res, dst, comps, caps, "period skew %d" % skew)
+        assert all(res["status"] == 0)
+
+
+@pytest.mark.parametrize("fmt", ["lz4", "snappy"])
 def test_mutants_match_oracle(cuda, fmt):
     rng = random.Random(9)
     raws = gen([50, 3000, 40000, 70000], probs=[0.3, 0.5, 0.7, 0.5], seed=4)
