@@ -52,6 +52,11 @@ SIGNATURES = {
     "cudec_version": (ctypes.c_int, []),
     "cudec_lz4_decompress_batch": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P]),
     "cudec_snappy_decompress_batch": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P]),
+    "cudec_lz4f_decompress": (ctypes.c_int, [_P, _SZ, _P, _SZ, _P]),
+    "cudec_stream_ctx_create": (ctypes.c_int, [_P]),
+    "cudec_lz4_decompress_stream_ctx": (ctypes.c_int, [_P, _P, _P, _P, _P, _SZ, ctypes.c_int, _P]),
+    "cudec_stream_ctx_destroy": (None, [_P]),
+    "cudec_lz4_decompress_stream": (ctypes.c_int, [_P, _P, _P, _P, _SZ, ctypes.c_int, _P]),
 }
 
 _lib = None
@@ -101,3 +106,41 @@ BATCH_ENTRIES = {
     "lz4": lz4_decompress_batch,
     "snappy": snappy_decompress_batch,
 }
+
+
+def lz4f_decompress(frame, dst_capacity):
+    """cudec_lz4f_decompress over Python bytes: returns (status, bytes)."""
+    import numpy as np
+    src = np.frombuffer(bytes(frame) if frame else b"\0", dtype=np.uint8)
+    out = np.zeros(max(dst_capacity, 1), dtype=np.uint8)
+    written = ctypes.c_size_t(0)
+    st = lib().cudec_lz4f_decompress(src.ctypes.data, len(frame), out.ctypes.data,
+                                      dst_capacity, ctypes.byref(written))
+    return st, out[:written.value].tobytes()
+
+
+class StreamContext:
+    """cudec_stream_ctx: create / decode (host arrays) / destroy."""
+
+    def __init__(self):
+        h = ctypes.c_void_p()
+        st = lib().cudec_stream_ctx_create(ctypes.byref(h))
+        if st != OK:
+            raise RuntimeError("cudec_stream_ctx_create: %s" % STATUS_NAMES.get(st, st))
+        self.handle = h
+
+    def decode(self, src_ptrs, src_sizes, dst_ptrs, dst_caps, n, space, results):
+        """All arguments are host addresses of arrays (ints); returns status."""
+        return lib().cudec_lz4_decompress_stream_ctx(self.handle, src_ptrs, src_sizes,
+                                                     dst_ptrs, dst_caps, n, space, results)
+
+    def close(self):
+        if self.handle:
+            lib().cudec_stream_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,319 @@
+// Pinned streaming decode context: host-resident compressed chunks in,
+// device- or host-resident output, synchronous.
+//
+// Replaces iderex/cudec src/stream.cpp:42-593 with the same contract
+// (argument rules, wave sizing by a staging budget and a chunk ceiling,
+// grow-only staging, per-chunk records always defined, aggregate status = CUDA
+// fault first, else the first non-OK chunk in index order, poison latch on a
+// CUDA fault). The data path differs: the staging is double-buffered, so the
+// host copies wave w+1's chunks into pinned memory while the device uploads,
+// decodes and reads back wave w; host-side output comes back as one copy of
+// the wave's staging into pinned memory and is scattered to the caller's
+// buffers (exactly bytes_written each) while the next wave is on the device.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "cudec.h"
+#include "host_util.h"
+#include "launch.h"
+
+namespace {
+
+// Staging per wave: compressed bytes (+ host-output destination bytes) are
+// charged at the largest chunk of the call, as the reference's sizer does
+// (src/stream.cpp:58-105); two waves are staged at a time.
+constexpr size_t kWaveBudget = size_t{192} << 20;
+constexpr size_t kWaveChunksMax = 4096;
+
+size_t choose_wave(const size_t* sizes, const size_t* caps, size_t n, bool host_out) {
+    size_t per = 1;
+    for (size_t i = 0; i < n; ++i) {
+        size_t b = sizes[i];
+        if (host_out) b = (SIZE_MAX - b < caps[i]) ? SIZE_MAX : b + caps[i];
+        if (b > per) per = b;
+    }
+    size_t w = kWaveBudget / per;
+    if (w == 0) w = 1;
+    if (w > kWaveChunksMax) w = kWaveChunksMax;
+    if (w > n) w = n;
+    return w;
+}
+
+void stamp(cudec_chunk_result* r, size_t n, cudec_status st) {
+    for (size_t i = 0; i < n; ++i) {
+        r[i].status = static_cast<int32_t>(st);
+        r[i].reserved = 0;
+        r[i].bytes_written = 0;
+    }
+}
+
+// Same rules as src/stream.cpp:182-201; no CUDA call.
+cudec_status validate(const void* const* src, const size_t* sizes, void* const* dst,
+                      const size_t* caps, size_t n, cudec_mem_space space,
+                      const cudec_chunk_result* res) {
+    if (src == nullptr || sizes == nullptr || dst == nullptr || caps == nullptr ||
+        res == nullptr || n == 0 || n > cdb::kMaxBatchChunks ||
+        (space != CUDEC_MEM_HOST && space != CUDEC_MEM_DEVICE))
+        return CUDEC_ERR_INVALID_ARGUMENT;
+    for (size_t i = 0; i < n; ++i)
+        if ((src[i] == nullptr && sizes[i] != 0) || (dst[i] == nullptr && caps[i] != 0))
+            return CUDEC_ERR_INVALID_ARGUMENT;
+    return CUDEC_OK;
+}
+
+}  // namespace
+
+struct cudec_stream_ctx {
+    cdb::StreamOwner stream;
+    cdb::EventOwner drained[2];  // slot b's wave is done (staging reusable)
+    cdb::PinnedBuf p_src[2], p_meta[2], p_out[2];
+    cdb::DevBuf d_src[2], d_meta[2], d_out[2];
+    cdb::DevBuf d_results;
+    cdb::PinnedBuf p_results;
+    bool poisoned = false;
+};
+
+namespace {
+
+// Copy one drained host-output wave from pinned staging to the caller:
+// exactly bytes_written per chunk, bounded by the chunk's capacity (a longer
+// device-reported length is a device fault: the chunk is stamped CUDA and
+// the wave fails, as src/stream.cpp:163-184 does).
+cudec_status scatter_wave(cudec_chunk_result* wr, const unsigned char* staged,
+                          void* const* dst, const size_t* caps, size_t begin, size_t wn) {
+    size_t off = 0;
+    for (size_t j = 0; j < wn; ++j) {
+        const size_t i = begin + j;
+        const size_t bw = static_cast<size_t>(wr[j].bytes_written);
+        if (bw > caps[i]) {
+            wr[j].status = CUDEC_ERR_CUDA;
+            wr[j].reserved = 0;
+            wr[j].bytes_written = 0;
+            return CUDEC_ERR_CUDA;
+        }
+        if (bw != 0 && dst[i] != nullptr) std::memcpy(dst[i], staged + off, bw);
+        off += caps[i];
+    }
+    return CUDEC_OK;
+}
+
+cudec_status decode(cudec_stream_ctx& ctx, const void* const* src, const size_t* sizes,
+                    void* const* dst, const size_t* caps, size_t n, cudec_mem_space space,
+                    cudec_chunk_result* results) {
+    const bool host_out = space == CUDEC_MEM_HOST;
+    const size_t wave = choose_wave(sizes, caps, n, host_out);
+    const size_t waves = (n + wave - 1) / wave;
+    stamp(results, n, CUDEC_ERR_CUDA);
+
+    size_t max_src = 0, max_out = 0;
+    for (size_t w = 0; w < waves; ++w) {
+        const size_t b = w * wave, e = b + wave < n ? b + wave : n;
+        size_t ws = 0, wo = 0;
+        for (size_t i = b; i < e; ++i) {
+            if (SIZE_MAX - ws < sizes[i]) return CUDEC_ERR_CORRUPT_INPUT;
+            ws += sizes[i];
+            if (host_out) {
+                if (SIZE_MAX - wo < caps[i]) return CUDEC_ERR_CORRUPT_INPUT;
+                wo += caps[i];
+            }
+        }
+        if (ws > max_src) max_src = ws;
+        if (wo > max_out) max_out = wo;
+    }
+    if (n > SIZE_MAX / sizeof(cudec_chunk_result)) return CUDEC_ERR_CORRUPT_INPUT;
+    const size_t meta_bytes = 4 * wave * sizeof(uint64_t);
+    const size_t res_bytes = n * sizeof(cudec_chunk_result);
+#define GROW(call)                       \
+    do {                                 \
+        if ((call) != cudaSuccess) {     \
+            (void)cudaGetLastError();    \
+            ctx.poisoned = true;         \
+            return CUDEC_ERR_CUDA;       \
+        }                                \
+    } while (0)
+    const size_t slots = waves > 1 ? 2 : 1;
+    for (size_t b = 0; b < slots; ++b) {
+        GROW(ctx.p_src[b].ensure(max_src ? max_src : 1));
+        GROW(ctx.d_src[b].ensure(max_src ? max_src : 1));
+        GROW(ctx.p_meta[b].ensure(meta_bytes));
+        GROW(ctx.d_meta[b].ensure(meta_bytes));
+        if (host_out) {
+            GROW(ctx.d_out[b].ensure(max_out ? max_out : 1));
+            GROW(ctx.p_out[b].ensure(max_out ? max_out : 1));
+        }
+    }
+    GROW(ctx.d_results.ensure(res_bytes));
+    GROW(ctx.p_results.ensure(res_bytes));
+#undef GROW
+    cudaStream_t s = ctx.stream.s;
+    cudec_chunk_result* p_res = static_cast<cudec_chunk_result*>(ctx.p_results.p);
+    stamp(p_res, n, CUDEC_ERR_CUDA);
+
+    cudec_status fail = CUDEC_OK;
+    bool slot_busy[2] = {false, false};
+    size_t slot_begin[2] = {0, 0}, slot_n[2] = {0, 0};
+    // Host-output: finish (scatter) the wave staged in `slot`.
+    auto finish_slot = [&](int slot) -> cudec_status {
+        if (!slot_busy[slot]) return CUDEC_OK;
+        if (cudaEventSynchronize(ctx.drained[slot].e) != cudaSuccess) return CUDEC_ERR_CUDA;
+        slot_busy[slot] = false;
+        if (!host_out) return CUDEC_OK;
+        return scatter_wave(p_res + slot_begin[slot],
+                            static_cast<const unsigned char*>(ctx.p_out[slot].p), dst, caps,
+                            slot_begin[slot], slot_n[slot]);
+    };
+    for (size_t w = 0; w < waves && fail == CUDEC_OK; ++w) {
+        const int b = static_cast<int>(w & 1);
+        const size_t begin = w * wave, end = begin + wave < n ? begin + wave : n;
+        const size_t wn = end - begin;
+        // The slot's previous wave must be fully out of its staging.
+        if ((fail = finish_slot(b)) != CUDEC_OK) break;
+        unsigned char* ps = static_cast<unsigned char*>(ctx.p_src[b].p);
+        unsigned char* ds = static_cast<unsigned char*>(ctx.d_src[b].p);
+        unsigned char* dout = static_cast<unsigned char*>(ctx.d_out[b].p);
+        uint64_t* pm = static_cast<uint64_t*>(ctx.p_meta[b].p);
+        size_t so = 0, oo = 0;
+        for (size_t j = 0; j < wn; ++j) {
+            const size_t i = begin + j;
+            if (sizes[i]) std::memcpy(ps + so, src[i], sizes[i]);
+            pm[j] = reinterpret_cast<uint64_t>(ds + so);
+            pm[wave + j] = sizes[i];
+            pm[2 * wave + j] = host_out ? reinterpret_cast<uint64_t>(dout + oo)
+                                        : reinterpret_cast<uint64_t>(dst[i]);
+            pm[3 * wave + j] = caps[i];
+            so += sizes[i];
+            if (host_out) oo += caps[i];
+        }
+        if (so && cudaMemcpyAsync(ds, ps, so, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+            fail = CUDEC_ERR_CUDA;
+            break;
+        }
+        if (cudaMemcpyAsync(ctx.d_meta[b].p, pm, meta_bytes, cudaMemcpyHostToDevice, s) !=
+            cudaSuccess) {
+            fail = CUDEC_ERR_CUDA;
+            break;
+        }
+        const uint64_t* dm = static_cast<const uint64_t*>(ctx.d_meta[b].p);
+        cudec_chunk_result* d_res = static_cast<cudec_chunk_result*>(ctx.d_results.p) + begin;
+        const cudec_status launched = cudec_lz4_decompress_batch(
+            reinterpret_cast<const void* const*>(dm), reinterpret_cast<const size_t*>(dm + wave),
+            reinterpret_cast<void* const*>(dm + 2 * wave),
+            reinterpret_cast<const size_t*>(dm + 3 * wave), wn, d_res, s);
+        if (launched != CUDEC_OK) {
+            fail = launched;
+            break;
+        }
+        if (cudaMemcpyAsync(p_res + begin, d_res, wn * sizeof(cudec_chunk_result),
+                            cudaMemcpyDeviceToHost, s) != cudaSuccess) {
+            fail = CUDEC_ERR_CUDA;
+            break;
+        }
+        if (host_out && oo &&
+            cudaMemcpyAsync(ctx.p_out[b].p, dout, oo, cudaMemcpyDeviceToHost, s) != cudaSuccess) {
+            fail = CUDEC_ERR_CUDA;
+            break;
+        }
+        if (cudaEventRecord(ctx.drained[b].e, s) != cudaSuccess) {
+            fail = CUDEC_ERR_CUDA;
+            break;
+        }
+        slot_busy[b] = true;
+        slot_begin[b] = begin;
+        slot_n[b] = wn;
+    }
+    // Drain: no work outlives the call.
+    cudec_status drain = fail;
+    if (cudaStreamSynchronize(s) != cudaSuccess && drain == CUDEC_OK) drain = CUDEC_ERR_CUDA;
+    if (cudaGetLastError() != cudaSuccess && drain == CUDEC_OK) drain = CUDEC_ERR_CUDA;
+    if (drain == CUDEC_OK) {
+        // finish in wave order (the older slot first)
+        const int first = waves > 1 ? static_cast<int>((waves - 2) & 1) : 0;
+        for (int k = 0; k < 2 && drain == CUDEC_OK; ++k) {
+            const int slot = (first + k) & 1;
+            drain = finish_slot(slot);
+        }
+    }
+    if (drain != CUDEC_OK && host_out) {
+        // Waves whose output never reached the caller are not decodes.
+        for (int slot = 0; slot < 2; ++slot)
+            if (slot_busy[slot]) stamp(p_res + slot_begin[slot], slot_n[slot], CUDEC_ERR_CUDA);
+    }
+    std::memcpy(results, p_res, res_bytes);
+    if (drain != CUDEC_OK) {
+        ctx.poisoned = true;
+        return drain;
+    }
+    for (size_t i = 0; i < n; ++i)
+        if (results[i].status != CUDEC_OK) return static_cast<cudec_status>(results[i].status);
+    return CUDEC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+cudec_status cudec_stream_ctx_create(cudec_stream_ctx** out_ctx) {
+    if (out_ctx == nullptr) return CUDEC_ERR_INVALID_ARGUMENT;
+    *out_ctx = nullptr;
+    cudec_stream_ctx* ctx = new (std::nothrow) cudec_stream_ctx();
+    if (ctx == nullptr) return CUDEC_ERR_CUDA;
+    if (ctx->stream.create() != cudaSuccess || ctx->drained[0].create() != cudaSuccess ||
+        ctx->drained[1].create() != cudaSuccess) {
+        (void)cudaGetLastError();
+        delete ctx;
+        return CUDEC_ERR_CUDA;
+    }
+    *out_ctx = ctx;
+    return CUDEC_OK;
+}
+
+cudec_status cudec_lz4_decompress_stream_ctx(cudec_stream_ctx* ctx,
+                                             const void* const* h_src_ptrs,
+                                             const size_t* h_src_sizes, void* const* dst_ptrs,
+                                             const size_t* dst_caps, size_t chunk_count,
+                                             cudec_mem_space dst_space,
+                                             cudec_chunk_result* h_results) {
+    if (ctx == nullptr) return CUDEC_ERR_INVALID_ARGUMENT;
+    const cudec_status a = validate(h_src_ptrs, h_src_sizes, dst_ptrs, dst_caps, chunk_count,
+                                    dst_space, h_results);
+    if (a != CUDEC_OK) return a;
+    if (ctx->poisoned) {
+        stamp(h_results, chunk_count, CUDEC_ERR_CUDA);
+        return CUDEC_ERR_CUDA;
+    }
+    try {
+        return decode(*ctx, h_src_ptrs, h_src_sizes, dst_ptrs, dst_caps, chunk_count, dst_space,
+                      h_results);
+    } catch (...) {
+        ctx->poisoned = true;
+        return CUDEC_ERR_CUDA;
+    }
+}
+
+void cudec_stream_ctx_destroy(cudec_stream_ctx* ctx) {
+    if (ctx == nullptr) return;
+    if (ctx->stream.s != nullptr) (void)cudaStreamSynchronize(ctx->stream.s);
+    delete ctx;
+}
+
+cudec_status cudec_lz4_decompress_stream(const void* const* h_src_ptrs,
+                                         const size_t* h_src_sizes, void* const* dst_ptrs,
+                                         const size_t* dst_caps, size_t chunk_count,
+                                         cudec_mem_space dst_space,
+                                         cudec_chunk_result* h_results) {
+    const cudec_status a = validate(h_src_ptrs, h_src_sizes, dst_ptrs, dst_caps, chunk_count,
+                                    dst_space, h_results);
+    if (a != CUDEC_OK) return a;
+    cudec_stream_ctx* ctx = nullptr;
+    const cudec_status c = cudec_stream_ctx_create(&ctx);
+    if (c != CUDEC_OK) return c;
+    const cudec_status st = cudec_lz4_decompress_stream_ctx(
+        ctx, h_src_ptrs, h_src_sizes, dst_ptrs, dst_caps, chunk_count, dst_space, h_results);
+    cudec_stream_ctx_destroy(ctx);
+    return st;
+}
+
+}  // extern "C"

@@ -139,3 +139,42 @@ def snappy_decompress_ref(comp, declared):
                                          asbytes=True)
     except Exception:  # pyarrow raises on any malformed stream
         return None
+
+
+class _LZ4FPrefs(ctypes.Structure):
+    # LZ4F_preferences_t (lz4frame.h): frameInfo {blockSizeID, blockMode,
+    # contentChecksumFlag, frameType, contentSize, dictID, blockChecksumFlag},
+    # compressionLevel, autoFlush, favorDecSpeed, reserved[3].
+    _fields_ = [("blockSizeID", ctypes.c_int), ("blockMode", ctypes.c_int),
+                ("contentChecksumFlag", ctypes.c_int), ("frameType", ctypes.c_int),
+                ("contentSize", ctypes.c_ulonglong), ("dictID", ctypes.c_uint),
+                ("blockChecksumFlag", ctypes.c_int), ("compressionLevel", ctypes.c_int),
+                ("autoFlush", ctypes.c_uint), ("favorDecSpeed", ctypes.c_uint),
+                ("reserved", ctypes.c_uint * 3)]
+
+
+def lz4f_compress(data, block_size_id=4, independent=True, content_checksum=False,
+                  block_checksum=False, content_size=False, level=0):
+    """One .lz4 frame via liblz4 LZ4F_compressFrame."""
+    L = _lz4lib()
+    data = bytes(data)
+    prefs = _LZ4FPrefs()
+    prefs.blockSizeID = block_size_id
+    prefs.blockMode = 1 if independent else 0
+    prefs.contentChecksumFlag = 1 if content_checksum else 0
+    prefs.blockChecksumFlag = 1 if block_checksum else 0
+    prefs.contentSize = len(data) if content_size else 0
+    prefs.compressionLevel = level
+    L.LZ4F_compressFrameBound.restype = ctypes.c_size_t
+    L.LZ4F_compressFrameBound.argtypes = [ctypes.c_size_t, ctypes.c_void_p]
+    L.LZ4F_compressFrame.restype = ctypes.c_size_t
+    L.LZ4F_compressFrame.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
+                                     ctypes.c_size_t, ctypes.c_void_p]
+    L.LZ4F_isError.restype = ctypes.c_uint
+    L.LZ4F_isError.argtypes = [ctypes.c_size_t]
+    bound = L.LZ4F_compressFrameBound(len(data), ctypes.byref(prefs))
+    out = ctypes.create_string_buffer(bound)
+    n = L.LZ4F_compressFrame(out, bound, data, len(data), ctypes.byref(prefs))
+    if L.LZ4F_isError(n):
+        raise RuntimeError("LZ4F_compressFrame failed")
+    return out.raw[:n]

@@ -114,6 +114,73 @@ cudec_status cudec_snappy_decompress_batch(const void* const* d_src_ptrs,
                                            cudec_chunk_result* d_results,
                                            cudec_stream_t stream);
 
+/* ---------------------------------------------------------------------
+ * LZ4 frame (.lz4 container), host memory in and out, synchronous.
+ * Replaces: include/cudec.h:130-132, src/frame.cpp:401-422.
+ *
+ * Decodes block-INDEPENDENT frames; verifies the header, block and content
+ * checksums and the declared content size when present. Returns
+ * CUDEC_ERR_UNSUPPORTED for a valid frame outside that subset (block-linked
+ * mode, a dictionary id), CUDEC_ERR_CORRUPT_INPUT for a malformed frame or a
+ * checksum / content-size mismatch, CUDEC_ERR_OUTPUT_TOO_SMALL when
+ * dst_capacity is short, CUDEC_ERR_CUDA on a device or host resource failure,
+ * and CUDEC_ERR_INVALID_ARGUMENT for a NULL frame or bytes_written, or a NULL
+ * dst with a non-zero capacity. On any error *bytes_written is 0.
+ * ------------------------------------------------------------------- */
+cudec_status cudec_lz4f_decompress(const void* frame, size_t frame_size,
+                                   void* dst, size_t dst_capacity,
+                                   size_t* bytes_written);
+
+/* Memory space of the streaming decoder's destinations.
+ * Replaces: include/cudec.h:135-138. */
+typedef enum cudec_mem_space {
+    CUDEC_MEM_HOST = 0,   /* host destinations; output is copied back */
+    CUDEC_MEM_DEVICE = 1  /* device destinations; output stays in HBM */
+} cudec_mem_space;
+
+/* ---------------------------------------------------------------------
+ * Streaming batch LZ4 block decode from HOST-resident chunks.
+ * Replaces: include/cudec.h:140-218, src/stream.cpp:492-593.
+ *
+ * A context owns a CUDA stream and grow-only pinned/device staging (sized to
+ * the largest batch so far); create it once per thread and reuse it. It is
+ * not thread-safe. Decoding is synchronous: every destination and result is
+ * final on return. Argument arrays are host arrays of chunk_count entries;
+ * dst_ptrs are host or device pointers per dst_space; exactly bytes_written
+ * bytes are written per successful chunk, in both spaces.
+ *
+ * A NULL ctx or array, a NULL source with a non-zero size, a NULL
+ * destination with a non-zero capacity, an unknown dst_space, chunk_count ==
+ * 0 or above the launch limit: CUDEC_ERR_INVALID_ARGUMENT, nothing decoded,
+ * the context not poisoned, h_results untouched. Otherwise every record is
+ * defined on return; the aggregate is CUDEC_OK iff every chunk decoded, else
+ * CUDEC_ERR_CUDA if a device/host resource failure happened, else the first
+ * non-OK chunk's status in index order. A CUDA fault poisons the context:
+ * every later decode returns CUDEC_ERR_CUDA without touching the device;
+ * only destroy is valid on it. Nothing throws across this boundary.
+ * ------------------------------------------------------------------- */
+typedef struct cudec_stream_ctx cudec_stream_ctx;
+
+cudec_status cudec_stream_ctx_create(cudec_stream_ctx** out_ctx);
+
+cudec_status cudec_lz4_decompress_stream_ctx(
+    cudec_stream_ctx* ctx, const void* const* h_src_ptrs,
+    const size_t* h_src_sizes, void* const* dst_ptrs, const size_t* dst_caps,
+    size_t chunk_count, cudec_mem_space dst_space,
+    cudec_chunk_result* h_results);
+
+/* NULL-safe; valid on a poisoned context. */
+void cudec_stream_ctx_destroy(cudec_stream_ctx* ctx);
+
+/* One-shot: create, one decode, destroy (pays the staging every call). */
+cudec_status cudec_lz4_decompress_stream(const void* const* h_src_ptrs,
+                                         const size_t* h_src_sizes,
+                                         void* const* dst_ptrs,
+                                         const size_t* dst_caps,
+                                         size_t chunk_count,
+                                         cudec_mem_space dst_space,
+                                         cudec_chunk_result* h_results);
+
 #ifdef __cplusplus
 }
 #endif

@@ -53,6 +53,7 @@ def oracle_lib():
     h = _load(ORACLE_LIB, {
         "oracle_lz4_decode": (ctypes.c_int, _DEC),
         "oracle_snappy_decode": (ctypes.c_int, _DEC),
+        "oracle_lz4f_decode": (ctypes.c_int, _DEC),
         "oracle_lz4_decode_batch": (ctypes.c_int, _BATCH),
         "oracle_snappy_decode_batch": (ctypes.c_int, _BATCH),
         "codec_decode_batch": (ctypes.c_int, [ctypes.c_int] + _BATCH),
@@ -81,6 +82,9 @@ def ref_gpu_lib():
                                        [ctypes.c_size_t, ctypes.c_void_p,
                                         ctypes.c_void_p]),
         "cudec_version": (ctypes.c_int, []),
+        "cudec_lz4f_decompress": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t,
+                                                 ctypes.c_void_p, ctypes.c_size_t,
+                                                 ctypes.c_void_p]),
     })
 
 
@@ -97,6 +101,25 @@ def _decode_one(fn, comp, cap):
 def lz4_decode(comp, cap):
     """(status, bytes) from the C restatement."""
     return _decode_one(oracle_lib().oracle_lz4_decode, comp, cap)
+
+
+def lz4f_decode(frame, cap):
+    """(status, bytes) from the C restatement of the frame ladder."""
+    return _decode_one(oracle_lib().oracle_lz4f_decode, frame, cap)
+
+
+def ref_lz4f_decode(frame, cap):
+    """(status, bytes) from the reference library's own frame entry (GPU),
+    or None where it was not built."""
+    h = ref_gpu_lib()
+    if h is None:
+        return None
+    src = np.frombuffer(bytes(frame) if frame else b"\0", dtype=np.uint8)
+    out = np.zeros(max(cap, 1), dtype=np.uint8)
+    w = ctypes.c_size_t(0)
+    st = h.cudec_lz4f_decompress(src.ctypes.data, len(frame), out.ctypes.data, cap,
+                                 ctypes.byref(w))
+    return st, out[:w.value].tobytes()
 
 
 def snappy_decode(comp, cap):

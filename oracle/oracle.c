@@ -21,6 +21,7 @@
 #include <stdatomic.h>
 #include <stddef.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 enum {
@@ -237,4 +238,133 @@ int oracle_snappy_decode_batch(const uint8_t* const* src,
                                uint64_t* written, int threads) {
     return run_batch(oracle_snappy_decode, src, src_sizes, dst, caps, n, status,
                      written, threads);
+}
+
+/* ------------------------------------------------------------------------
+ * LZ4 frame. Follows src/frame.cpp:282-397 (DecodeFrame) and :53-278
+ * (DecodeAndAssemble: every block reject is CORRUPT; capacity checked before
+ * any byte is placed). XXH32 restated from the public xxHash specification.
+ * ---------------------------------------------------------------------- */
+
+static uint32_t o_rotl(uint32_t x, int r) { return (x << r) | (x >> (32 - r)); }
+static uint32_t o_rd32(const uint8_t* p) {
+    return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) |
+           ((uint32_t)p[3] << 24);
+}
+
+uint32_t oracle_xxh32(const uint8_t* p, uint64_t len, uint32_t seed) {
+    const uint32_t P1 = 2654435761u, P2 = 2246822519u, P3 = 3266489917u,
+                   P4 = 668265263u, P5 = 374761393u;
+    uint64_t i = 0;
+    uint32_t h;
+    if (len >= 16) {
+        uint32_t v[4] = {seed + P1 + P2, seed + P2, seed, seed - P1};
+        for (; i + 16 <= len; i += 16)
+            for (int k = 0; k < 4; k++) v[k] = o_rotl(v[k] + o_rd32(p + i + 4 * k) * P2, 13) * P1;
+        h = o_rotl(v[0], 1) + o_rotl(v[1], 7) + o_rotl(v[2], 12) + o_rotl(v[3], 18);
+    } else {
+        h = seed + P5;
+    }
+    h += (uint32_t)len;
+    for (; i + 4 <= len; i += 4) h = o_rotl(h + o_rd32(p + i) * P3, 17) * P4;
+    for (; i < len; i++) h = o_rotl(h + p[i] * P5, 11) * P1;
+    h ^= h >> 15;
+    h *= P2;
+    h ^= h >> 13;
+    h *= P3;
+    h ^= h >> 16;
+    return h;
+}
+
+int oracle_lz4f_decode(const uint8_t* f, uint64_t n, uint8_t* out, uint64_t cap,
+                       uint64_t* written) {
+    *written = 0;
+    if (n < 7 || o_rd32(f) != 0x184D2204u) return ST_CORRUPT;
+    const unsigned flg = f[4], bd = f[5];
+    if (((flg >> 6) & 3) != 1 || (flg & 2)) return ST_CORRUPT;
+    if (bd & 0x8F) return ST_CORRUPT;
+    const unsigned bmax = (bd >> 4) & 7;
+    if (bmax < 4 || bmax > 7) return ST_CORRUPT;
+    const uint64_t block_max = (uint64_t)65536 << ((bmax - 4) * 2);
+    if (!((flg >> 5) & 1) || (flg & 1)) return ST_UNSUPPORTED;
+    uint64_t pos = 6, declared = 0;
+    const int has_size = (flg >> 3) & 1, bsum = (flg >> 4) & 1, csum = (flg >> 2) & 1;
+    if (has_size) {
+        if (n < pos + 8) return ST_CORRUPT;
+        declared = (uint64_t)o_rd32(f + pos) | ((uint64_t)o_rd32(f + pos + 4) << 32);
+        pos += 8;
+    }
+    if (n < pos + 1) return ST_CORRUPT;
+    if (((oracle_xxh32(f + 4, pos - 4, 0) >> 8) & 0xFF) != f[pos]) return ST_CORRUPT;
+    pos++;
+    /* first pass: the block table with checksums (no output yet) */
+    uint64_t bpos = pos;
+    int end = 0;
+    for (uint64_t fuel = n / 4 + 1; fuel; fuel--) {
+        if (n < bpos + 4) return ST_CORRUPT;
+        const uint32_t bs = o_rd32(f + bpos);
+        bpos += 4;
+        if (bs == 0) { end = 1; break; }
+        const uint64_t blen = bs & 0x7FFFFFFFu;
+        if (blen == 0 || blen > block_max || n < bpos + blen) return ST_CORRUPT;
+        if (bsum) {
+            if (n < bpos + blen + 4) return ST_CORRUPT;
+            if (oracle_xxh32(f + bpos, blen, 0) != o_rd32(f + bpos + blen)) return ST_CORRUPT;
+        }
+        bpos += blen + (bsum ? 4 : 0);
+    }
+    if (!end) return ST_CORRUPT;
+    /* second pass: decode every compressed block into a scratch slot first
+     * (all block rejects win over the capacity check), then place. */
+    uint64_t total = 0;
+    int too_small = 0;
+    uint64_t p2 = pos;
+    uint8_t* scratch = (uint8_t*)malloc(block_max ? block_max : 1);
+    if (!scratch) return ST_CUDA;
+    /* pass 2a: validate all blocks and sum sizes */
+    for (;;) {
+        const uint32_t bs = o_rd32(f + p2);
+        p2 += 4;
+        if (bs == 0) break;
+        const uint64_t blen = bs & 0x7FFFFFFFu;
+        uint64_t len = blen;
+        if (!(bs >> 31)) {
+            uint64_t w = 0;
+            if (oracle_lz4_decode(f + p2, blen, scratch, block_max, &w) != ST_OK) {
+                free(scratch);
+                return ST_CORRUPT;
+            }
+            len = w;
+        }
+        if (len > cap - total) too_small = 1;
+        if (!too_small) total += len;
+        p2 += blen + (bsum ? 4 : 0);
+    }
+    if (too_small) { free(scratch); return ST_TOO_SMALL; }
+    /* pass 2b: place */
+    p2 = pos;
+    uint64_t off = 0;
+    for (;;) {
+        const uint32_t bs = o_rd32(f + p2);
+        p2 += 4;
+        if (bs == 0) break;
+        const uint64_t blen = bs & 0x7FFFFFFFu;
+        if (bs >> 31) {
+            memcpy(out + off, f + p2, blen);
+            off += blen;
+        } else {
+            uint64_t w = 0;
+            oracle_lz4_decode(f + p2, blen, out + off, cap - off < block_max ? cap - off : block_max, &w);
+            off += w;
+        }
+        p2 += blen + (bsum ? 4 : 0);
+    }
+    free(scratch);
+    if (has_size && declared != total) return ST_CORRUPT;
+    if (csum) {
+        if (n < bpos + 4) return ST_CORRUPT;
+        if (oracle_xxh32(out, total, 0) != o_rd32(f + bpos)) return ST_CORRUPT;
+    }
+    *written = total;
+    return ST_OK;
 }

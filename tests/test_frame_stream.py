@@ -1,0 +1,248 @@
+"""LZ4 frame entry and pinned streaming context.
+
+CPU: the oracle's frame ladder against liblz4 frames and crafted negatives;
+argument rules of the frame and stream entries (they make no CUDA call).
+GPU: cudec_lz4f_decompress against the oracle and the reference library's
+own frame entry; the stream context against the batch path, fresh vs reused,
+both memory spaces, several waves, and the poison latch (a host-side
+allocation failure, no GPU fault) as in the reference's
+tests/stream_twin.cu:392-450.
+"""
+import ctypes
+import random
+import struct
+
+import numpy as np
+import pytest
+
+import cudec_b200 as cd
+import oracle
+from cudec_b200 import workload as W
+
+
+def raw_data(n, seed=1, p=0.5):
+    buf, _ = W.generate([n], W.lz_params(p), seeds=np.array([seed], dtype=np.uint64))
+    return buf.tobytes()
+
+
+FRAME_OPTS = [dict(), dict(content_checksum=True), dict(block_checksum=True),
+              dict(content_size=True), dict(block_size_id=5, content_checksum=True),
+              dict(block_size_id=6, block_checksum=True, content_size=True),
+              dict(block_size_id=7)]
+
+
+def frames():
+    out = []
+    for i, kw in enumerate(FRAME_OPTS):
+        for n in (0, 1, 5000, 70000, 300000):
+            d = raw_data(n, seed=10 * i + 1) if n else b""
+            out.append((d, W.lz4f_compress(d, **kw), kw))
+    # incompressible content gives uncompressed (raw) blocks
+    rnd = np.random.default_rng(3).integers(0, 256, 200000, dtype=np.uint8).tobytes()
+    out.append((rnd, W.lz4f_compress(rnd, content_checksum=True), {"raw": True}))
+    return out
+
+
+def negatives(data, frame):
+    """Crafted frame negatives (the reference's tests/frame_host_negative.cpp
+    shapes): each entry (name, bytes, capacity)."""
+    f = bytearray(frame)
+    neg = [("empty", b"", 100), ("short", frame[:6], 100),
+           ("bad-magic", b"\x05" + frame[1:], len(data))]
+    g = bytearray(f); g[4] ^= 0x40; neg.append(("version", bytes(g), len(data)))
+    g = bytearray(f); g[4] |= 0x02; neg.append(("reserved-flg", bytes(g), len(data)))
+    g = bytearray(f); g[5] |= 0x80; neg.append(("reserved-bd", bytes(g), len(data)))
+    g = bytearray(f); g[5] = (g[5] & 0x8F) | 0x30; neg.append(("bmax-small", bytes(g), len(data)))
+    g = bytearray(f); g[-5] ^= 1; neg.append(("flip-late", bytes(g), len(data)))
+    g = bytearray(f); g[6] ^= 0xFF; neg.append(("header-checksum", bytes(g), len(data)))
+    neg.append(("truncated", frame[:len(frame) // 2], len(data)))
+    neg.append(("no-end-mark", frame[:-4] if len(frame) > 11 else frame[:7], len(data)))
+    neg.append(("capacity-short", frame, max(len(data) - 1, 0)))
+    return neg
+
+
+def test_oracle_frame_decodes_liblz4_frames():
+    for d, fr, kw in frames():
+        st, out = oracle.lz4f_decode(fr, len(d))
+        assert st == 0 and out == d, kw
+    # block-linked (liblz4's default) and dictionary frames are out of subset
+    big = raw_data(300000)  # one-block frames are written independent anyway
+    assert oracle.lz4f_decode(W.lz4f_compress(big, independent=False), len(big))[0] == 6
+
+
+def test_oracle_frame_negatives_fail_closed():
+    d = raw_data(70000, seed=4)
+    fr = W.lz4f_compress(d, content_checksum=True, block_checksum=True, content_size=True)
+    for name, body, cap in negatives(d, fr):
+        st, out = oracle.lz4f_decode(body, cap)
+        assert st != 0, name
+        assert out == b""
+
+
+def test_frame_and_stream_argument_rules_without_gpu():
+    lib = cd.lib()
+    w = ctypes.c_size_t(7)
+    buf = ctypes.create_string_buffer(64)
+    assert lib.cudec_lz4f_decompress(None, 10, buf, 64, ctypes.byref(w)) == cd.ERR_INVALID_ARGUMENT
+    assert w.value == 0
+    assert lib.cudec_lz4f_decompress(buf, 10, buf, 64, None) == cd.ERR_INVALID_ARGUMENT
+    assert lib.cudec_lz4f_decompress(buf, 10, None, 64, ctypes.byref(w)) == cd.ERR_INVALID_ARGUMENT
+    assert lib.cudec_stream_ctx_create(None) == cd.ERR_INVALID_ARGUMENT
+    lib.cudec_stream_ctx_destroy(None)
+    arr = (ctypes.c_uint64 * 4)(ctypes.addressof(buf), 0, 0, 0)
+    sizes = (ctypes.c_uint64 * 4)(4, 0, 0, 0)
+    caps = (ctypes.c_uint64 * 4)(64, 0, 0, 0)
+    dsts = (ctypes.c_uint64 * 4)(ctypes.addressof(buf), 0, 0, 0)
+    res = (cd.ChunkResult * 4)()
+    one = lib.cudec_lz4_decompress_stream
+    assert one(None, sizes, dsts, caps, 1, 0, res) == cd.ERR_INVALID_ARGUMENT
+    assert one(arr, sizes, dsts, caps, 0, 0, res) == cd.ERR_INVALID_ARGUMENT
+    assert one(arr, sizes, dsts, caps, 1, 7, res) == cd.ERR_INVALID_ARGUMENT
+    assert one(arr, sizes, dsts, caps, 2**64 - 1, 0, res) == cd.ERR_INVALID_ARGUMENT
+    sizes[1] = 5   # NULL source with a non-zero size
+    assert one(arr, sizes, dsts, caps, 2, 0, res) == cd.ERR_INVALID_ARGUMENT
+    sizes[1] = 0
+    caps[1] = 9    # NULL destination with a non-zero capacity
+    assert one(arr, sizes, dsts, caps, 2, 0, res) == cd.ERR_INVALID_ARGUMENT
+    assert lib.cudec_lz4_decompress_stream_ctx(None, arr, sizes, dsts, caps, 1, 0, res) \
+        == cd.ERR_INVALID_ARGUMENT
+
+
+# ------------------------------------------------------------------ GPU ---
+
+@pytest.mark.gpu
+def test_frame_entry_matches_oracle_and_reference(cuda):
+    have_ref = oracle.ref_gpu_lib() is not None
+    for d, fr, kw in frames():
+        st, out = cd.lz4f_decompress(fr, len(d) + 13)
+        assert st == 0 and out == d, kw
+        if have_ref:
+            assert oracle.ref_lz4f_decode(fr, len(d) + 13) == (st, out)
+    d = raw_data(70000, seed=4)
+    fr = W.lz4f_compress(d, content_checksum=True, block_checksum=True, content_size=True)
+    cases = negatives(d, fr)
+    rng = random.Random(5)
+    for k in range(60):
+        g = bytearray(fr)
+        for _ in range(rng.randint(1, 3)):
+            g[rng.randrange(len(g))] ^= 1 << rng.randrange(8)
+        cases.append(("mutant%d" % k, bytes(g), len(d)))
+    big = raw_data(300000, seed=8)
+    cases.append(("linked", W.lz4f_compress(big, independent=False), len(big)))
+    for name, body, cap in cases:
+        want = oracle.lz4f_decode(body, cap)
+        got = cd.lz4f_decompress(body, cap)
+        assert got[0] == want[0], (name, got[0], want[0])
+        assert got[1] == want[1], name
+        if have_ref:
+            assert oracle.ref_lz4f_decode(body, cap)[0] == got[0], name
+
+
+def host_arrays(comps, caps, space, device=None):
+    """Host pointer tables for the stream entry; destinations host or device."""
+    import torch
+    n = len(comps)
+    srcs = [np.frombuffer(c if c else b"\0", dtype=np.uint8).copy() for c in comps]
+    src_ptrs = np.array([s.ctypes.data for s in srcs], dtype=np.uint64)
+    sizes = np.array([len(c) for c in comps], dtype=np.uint64)
+    capa = np.array(caps, dtype=np.uint64)
+    if space == cd.MEM_HOST:
+        dsts = [np.full(max(c, 1), 0xA5, dtype=np.uint8) for c in caps]
+        dst_ptrs = np.array([x.ctypes.data for x in dsts], dtype=np.uint64)
+    else:
+        dsts = [torch.full((max(c, 1),), 0xA5, dtype=torch.uint8, device=device) for c in caps]
+        dst_ptrs = np.array([x.data_ptr() for x in dsts], dtype=np.uint64)
+    res = np.zeros(n, dtype=[("status", "<i4"), ("reserved", "<u4"), ("bytes_written", "<u8")])
+    return srcs, src_ptrs, sizes, capa, dsts, dst_ptrs, res
+
+
+def run_stream(ctx, comps, caps, space, device=None):
+    srcs, sp, sz, cp, dsts, dp, res = host_arrays(comps, caps, space, device)
+    st = ctx.decode(sp.ctypes.data, sz.ctypes.data, dp.ctypes.data, cp.ctypes.data,
+                    len(comps), space, res.ctypes.data)
+    outs = []
+    for i, x in enumerate(dsts):
+        h = x if space == cd.MEM_HOST else x.cpu().numpy()
+        outs.append(h.tobytes())
+    return st, res, outs
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("space", [0, 1])
+def test_stream_context_matches_oracle_fresh_and_reused(cuda, space):
+    rng = random.Random(7)
+    raws = [raw_data(n, seed=i + 3) for i, n in enumerate([1, 100, 5000, 65536, 70000, 200000])]
+    comps = [W.lz4_compress(r) for r in raws]
+    caps = [len(r) + 9 for r in raws]
+    # a corrupt neighbour must not disturb the others
+    bad = bytearray(comps[3]); bad[len(bad) // 2] ^= 0x55
+    comps.append(bytes(bad)); caps.append(65536)
+    ctx = cd.StreamContext()
+    for rep in range(3):
+        st, res, outs = run_stream(ctx, comps, caps, space, cuda)
+        want_st = [oracle.lz4_decode(c, k) for c, k in zip(comps, caps)]
+        first_bad = next((w[0] for w in want_st if w[0] != 0), 0)
+        assert st == first_bad
+        for i, (ws, wb) in enumerate(want_st):
+            assert res[i]["status"] == ws
+            if ws == 0:
+                assert res[i]["bytes_written"] == len(wb)
+                assert outs[i][:len(wb)] == wb
+                assert outs[i][len(wb):] == b"\xa5" * (len(outs[i]) - len(wb))
+        # the reused context (same inputs again) is bit-identical, and so is
+        # a fresh one
+        st2, res2, outs2 = run_stream(ctx, comps, caps, space, cuda)
+        fresh = cd.StreamContext()
+        st3, res3, outs3 = run_stream(fresh, comps, caps, space, cuda)
+        fresh.close()
+        assert st2 == st3 == st
+        ok = [i for i, w in enumerate(want_st) if w[0] == 0]
+        assert all(outs2[i] == outs[i] and outs3[i] == outs[i] for i in ok)
+        # grow the staging between repetitions
+        comps.append(W.lz4_compress(raw_data(300000 + rep, seed=99 + rep)))
+        caps.append(300000 + rep)
+    ctx.close()
+
+
+@pytest.mark.gpu
+def test_stream_many_waves_and_one_shot(cuda):
+    n = 9000  # more than one 4096-chunk wave
+    raws = [raw_data(200 + (i % 50), seed=i) for i in range(n)]
+    comps = [W.lz4_compress(r) for r in raws]
+    caps = [len(r) for r in raws]
+    srcs, sp, sz, cp, dsts, dp, res = host_arrays(comps, caps, cd.MEM_HOST)
+    st = cd.lib().cudec_lz4_decompress_stream(sp.ctypes.data, sz.ctypes.data, dp.ctypes.data,
+                                              cp.ctypes.data, n, cd.MEM_HOST, res.ctypes.data)
+    assert st == 0
+    assert all(dsts[i][:len(raws[i])].tobytes() == raws[i] for i in range(n))
+
+
+@pytest.mark.gpu
+def test_stream_poison_latch_on_allocation_failure(cuda):
+    """An impossible host-output staging size makes the grow allocation fail
+    on the host side: CUDA status, every record defined, context poisoned,
+    later decodes refused without touching the device."""
+    ctx = cd.StreamContext()
+    comp = W.lz4_compress(raw_data(1000))
+    src = np.frombuffer(comp, dtype=np.uint8).copy()
+    dst = np.zeros(4096, dtype=np.uint8)
+    sp = np.array([src.ctypes.data], dtype=np.uint64)
+    sz = np.array([len(comp)], dtype=np.uint64)
+    dp = np.array([dst.ctypes.data], dtype=np.uint64)
+    cp = np.array([1 << 60], dtype=np.uint64)
+    res = np.zeros(1, dtype=[("status", "<i4"), ("reserved", "<u4"), ("bytes_written", "<u8")])
+    res["status"] = 77
+    assert ctx.decode(sp.ctypes.data, sz.ctypes.data, dp.ctypes.data, cp.ctypes.data, 1,
+                      cd.MEM_HOST, res.ctypes.data) == cd.ERR_CUDA
+    assert res[0]["status"] == cd.ERR_CUDA and res[0]["bytes_written"] == 0
+    cp[0] = 1000
+    res["status"] = 77
+    assert ctx.decode(sp.ctypes.data, sz.ctypes.data, dp.ctypes.data, cp.ctypes.data, 1,
+                      cd.MEM_HOST, res.ctypes.data) == cd.ERR_CUDA
+    assert res[0]["status"] == cd.ERR_CUDA
+    ctx.close()
+    # a fresh context is unaffected
+    ctx2 = cd.StreamContext()
+    assert ctx2.decode(sp.ctypes.data, sz.ctypes.data, dp.ctypes.data, cp.ctypes.data, 1,
+                       cd.MEM_HOST, res.ctypes.data) == 0
+    ctx2.close()
