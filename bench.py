@@ -15,13 +15,15 @@ L2, so L2 is flushed (a 256 MiB memset) before every timed launch and only
 the launch itself is bracketed by CUDA events on its stream.
 
   value     decompressed bytes / mean launch time (whole job: all ranks)
-  e2e       the same metric through the C ABI with host buffers: each step
-            copies the compressed chunks and the chunk tables host->device
-            from pinned memory, decodes, and reads the 16-byte results back
+  e2e       the same metric through the C ABI with host buffers:
+            cudec_lz4_decompress_stream_ctx with the compressed chunks in
+            pinned host memory and destinations in HBM (host->device copy,
+            decode and result readback inside the synchronous call)
   roofline  (compressed + decompressed bytes) per launch / launch time,
             against the measured HBM copy bandwidth
   cpu_baseline  the reference's own host decoder (its twin, compiled from
             its sources) on all host cores, same chunks
+  per_format    the same measurement for raw Snappy (same content)
 
 `--impl reference` times that reference CPU decoder alone, same metric.
 Multi-GPU: replicas (chunks are independent; no exchange step).
@@ -44,6 +46,7 @@ CONFIG_SEED = 0xC0DEC
 N_CHUNKS = 1024
 CHUNK = 65536
 METRIC = "decompressed GB/s per format + % HBM roofline; serve p50/p99 latency"
+WORKLOAD = "lz4 block batch decode, %d x 64 KiB chunks"
 
 
 def parse_args():
@@ -53,31 +56,33 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=10.0,
-                    help="CPU-baseline sample length")
+                    help="CPU-baseline sample length (0 skips the CPU leg)")
+    ap.add_argument("--chunks", type=int, default=N_CHUNKS,
+                    help="chunk count (the headline workload is 1024; smaller "
+                         "counts are for profiler captures)")
     return ap.parse_args()
 
 
-def workload():
+def workload(n, fmt="lz4"):
     from cudec_b200 import workload as W
-    seeds = np.array([W.chunk_seed(CONFIG_SEED, 1, i) for i in range(N_CHUNKS)],
+    seeds = np.array([W.chunk_seed(CONFIG_SEED, 1, i) for i in range(n)],
                      dtype=np.uint64)
-    buf, offs = W.generate([CHUNK] * N_CHUNKS, W.lz_params(0.5), seeds=seeds)
+    buf, offs = W.generate([CHUNK] * n, W.lz_params(0.5), seeds=seeds)
     raws = [buf[int(o):int(o) + CHUNK] for o in offs]
-    comps = [W.lz4_compress(r) for r in raws]
-    return raws, comps
+    comp = W.lz4_compress if fmt == "lz4" else W.snappy_compress
+    return raws, [comp(r) for r in raws]
 
 
 def peaks():
-    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
-        with open(path) as f:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             return float(json.load(f)["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
         return 6650.0, "fallback"
 
 
 def traffic_per_launch():
-    """dram bytes per launch from the committed ncu summary, if any."""
+    """DRAM bytes per launch from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", "lz4_batch_64KiBx1024.txt")
     try:
         for line in open(path):
@@ -155,16 +160,18 @@ def cpu_sample(kind, comps, caps, seconds, threads):
         el = time.perf_counter() - t0
         if el >= seconds:
             break
-    out = float(sum(caps)) * reps
-    return out / el / 1e9, used, reps
+    return float(sum(caps)) * reps / el / 1e9, used, reps
 
 
 def run_reference(args, rank):
+    """The reference's own CPU decoder (its host twin over its parser), on
+    all host cores, same chunks and metric. Rank 0 only."""
     if rank != 0:
         return
     import oracle
-    raws, comps = workload()
-    caps = [CHUNK] * N_CHUNKS
+    n = args.chunks
+    _, comps = workload(n)
+    caps = [CHUNK] * n
     kind = "ref_lz4" if oracle.ref_twin_lib() is not None else "oracle_lz4"
     threads = os.cpu_count() or 1
     hb = oracle.HostBatch(comps, caps)
@@ -177,24 +184,39 @@ def run_reference(args, rank):
         oracle.decode_batch(kind, hb, threads)
         times.append(time.perf_counter() - t0)
     total = sum(times)
-    out_bytes = float(sum(caps))
-    value = out_bytes * len(times) / total / 1e9
-    line = {
+    value = float(sum(caps)) * len(times) / total / 1e9
+    print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GB/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1e3 * total / len(times), 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-        "config": {"workload": "lz4 block batch decode, 1024 x 64 KiB chunks (64 MiB out)",
-                   "format": "lz4", "chunks": N_CHUNKS, "chunk_bytes": CHUNK,
-                   "l2": "host decode (no GPU)"},
+        "config": {"workload": WORKLOAD % n, "format": "lz4", "chunks": n,
+                   "chunk_bytes": CHUNK, "l2": "host decode (no GPU)"},
         "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": threads,
                          "kind": "reference" if kind == "ref_lz4" else "port",
-                         "sample": "whole batch (64 MiB) per step, tests/lz4_twin.h over "
+                         "sample": "whole batch per step: tests/lz4_twin.h over "
                                    "src/lz4_block.h on a std::thread pool"},
         "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line), flush=True)
+    }), flush=True)
+
+
+def time_device(torch, batch, fmt, stream, flush, steps, warmup):
+    """Mean launch time (ms) of the batch entry, L2 flushed before each."""
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            flush.zero_()
+            assert batch.run(fmt, stream) == 0
+        for k in range(steps):
+            flush.zero_()
+            starts[k].record(stream)
+            rc = batch.run(fmt, stream)
+            ends[k].record(stream)
+            assert rc == 0
+    stream.synchronize()
+    return sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / steps
 
 
 def main():
@@ -217,11 +239,12 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
     cd.lib()
-
-    raws, comps = workload()
-    caps = [CHUNK] * N_CHUNKS
+    n = args.chunks
+    warm = max(args.warmup, 3)
+    raws, comps = workload(n)
+    caps = [CHUNK] * n
     in_bytes = sum(len(c) for c in comps)
-    out_bytes = CHUNK * N_CHUNKS
+    out_bytes = CHUNK * n
     batch = DeviceBatch(comps, caps, device=dev, poison=None)
     stream = torch.cuda.Stream(dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -233,7 +256,7 @@ def main():
     res = batch.results()
     assert (res["status"] == 0).all() and (res["bytes_written"] == CHUNK).all()
     dst = batch.dst_host()
-    for i in range(0, N_CHUNKS, 97):
+    for i in range(0, n, 97):
         assert batch.output(i, dst, CHUNK) == raws[i].tobytes()
 
     def barrier():
@@ -241,104 +264,110 @@ def main():
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    def max_over_ranks(x):
+        if world > 1:
+            t = torch.tensor([x], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    barrier()
     with ClockSampler(local) as clocks:
-        with torch.cuda.stream(stream):
-            for _ in range(max(args.warmup, 3)):
-                flush.zero_()
-                batch.run("lz4", stream)
-            barrier()
-            for k in range(args.steps):
-                flush.zero_()
-                starts[k].record(stream)
-                rc = batch.run("lz4", stream)
-                ends[k].record(stream)
-                assert rc == 0
-            barrier()
-    kernel_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    mean_ms = sum(kernel_ms) / len(kernel_ms)
-    if world > 1:
-        t = torch.tensor([mean_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        mean_ms = float(t.item())
+        mean_ms = time_device(torch, batch, "lz4", stream, flush, args.steps, warm)
+        barrier()
+    mean_ms = max_over_ranks(mean_ms)
     value = world * out_bytes / (mean_ms * 1e-3) / 1e9
 
+    # ---- Snappy, same content -------------------------------------------
+    _, scomps = workload(n, "snappy")
+    sbatch = DeviceBatch(scomps, caps, device=dev, poison=None)
+    s_ms = max_over_ranks(time_device(torch, sbatch, "snappy", stream, flush,
+                                      max(args.steps // 4, 1), warm))
+    sres = sbatch.results()
+    assert (sres["status"] == 0).all()
+    s_in = sum(len(c) for c in scomps)
+    del sbatch
+
     # ---- end to end through the C ABI with host buffers ----------------
-    pinned_src = torch.empty(batch.d_src.numel(), dtype=torch.uint8).pin_memory()
-    pinned_src.copy_(batch.d_src.cpu())
-    meta_dev = torch.cat([batch.d_src_ptrs, batch.d_src_sizes, batch.d_dst_ptrs, batch.d_caps])
-    pinned_meta = meta_dev.cpu().pin_memory()
-    meta_dev2 = torch.empty_like(meta_dev)
-    n = N_CHUNKS
-    pinned_res = torch.empty(16 * n, dtype=torch.uint8).pin_memory()
-    e_starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    e_ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    with torch.cuda.stream(stream):
-        for k in range(max(args.warmup, 3) + args.steps):
-            flush.zero_()
-            if k >= max(args.warmup, 3):
-                e_starts[k - max(args.warmup, 3)].record(stream)
-            batch.d_src.copy_(pinned_src, non_blocking=True)
-            meta_dev2.copy_(pinned_meta, non_blocking=True)
-            p = meta_dev2.data_ptr()
-            rc = cd.lz4_decompress_batch(p, p + 8 * n, p + 16 * n, p + 24 * n, n,
-                                         batch.d_results.data_ptr(), stream.cuda_stream)
-            pinned_res.copy_(batch.d_results, non_blocking=True)
-            if k >= max(args.warmup, 3):
-                e_ends[k - max(args.warmup, 3)].record(stream)
-            assert rc == 0
-    stream.synchronize()
-    e2e_ms = sum(s.elapsed_time(e) for s, e in zip(e_starts, e_ends)) / args.steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    r2 = np.frombuffer(pinned_res.numpy().tobytes(), dtype=[("s", "<i4"), ("r", "<u4"), ("w", "<u8")])
-    assert (r2["s"] == 0).all()
+    # cudec_lz4_decompress_stream_ctx: compressed chunks in pinned host memory,
+    # destinations in HBM; the synchronous call covers the host->device copy,
+    # the decode and the 16-byte result readback, so it is timed with the
+    # host clock around the call (L2 flushed before each).
+    blob = b"".join(comps)
+    pinned_src = torch.empty(len(blob), dtype=torch.uint8).pin_memory()
+    pinned_src.numpy()[:] = np.frombuffer(blob, dtype=np.uint8)
+    sizes_h = np.array([len(c) for c in comps], dtype=np.uint64)
+    offs_h = np.zeros(n, dtype=np.uint64)
+    offs_h[1:] = np.cumsum(sizes_h[:-1])
+    src_ptrs_h = (offs_h + pinned_src.data_ptr()).astype(np.uint64)
+    dst_ptrs_h = batch.d_dst_ptrs.cpu().numpy().astype(np.uint64)
+    caps_h = np.array(caps, dtype=np.uint64)
+    res_h = np.zeros(n, dtype=[("s", "<i4"), ("r", "<u4"), ("w", "<u8")])
+    batch.d_dst.fill_(0)
+    ctx = cd.StreamContext()
+    e2e_times = []
+    for k in range(warm + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        rc = ctx.decode(src_ptrs_h.ctypes.data, sizes_h.ctypes.data, dst_ptrs_h.ctypes.data,
+                        caps_h.ctypes.data, n, cd.MEM_DEVICE, res_h.ctypes.data)
+        t1 = time.perf_counter()
+        assert rc == 0 and (res_h["s"] == 0).all()
+        if k >= warm:
+            e2e_times.append(t1 - t0)
+    ctx.close()
+    e2e_ms = max_over_ranks(1e3 * sum(e2e_times) / len(e2e_times))
+    dst = batch.dst_host()
+    for i in range(0, n, 101):
+        assert batch.output(i, dst, CHUNK) == raws[i].tobytes()
     e2e = world * out_bytes / (e2e_ms * 1e-3) / 1e9
 
     peak, peak_kind = peaks()
     achieved = (in_bytes + out_bytes) / (mean_ms * 1e-3) / 1e9
-    line = None
     if rank == 0:
-        cpu = {}
-        if world == 1:
-            import oracle
-            kind = "ref_lz4" if oracle.ref_twin_lib() is not None else "oracle_lz4"
-            threads = os.cpu_count() or 1
-            v, used, reps = cpu_sample(kind, comps, caps, args.cpu_seconds, threads)
-            cpu = {"value": round(v, 3), "unit": "GB/s", "cores": used,
-                   "kind": "reference" if kind == "ref_lz4" else "port",
-                   "sample": "%d passes over the same 1024 x 64 KiB batch (~%.0f s), "
-                             "reference twin tests/lz4_twin.h on a std::thread pool"
-                             % (reps, args.cpu_seconds)}
-            cv, cused, creps = cpu_sample("codec_lz4", comps, caps, min(args.cpu_seconds, 5.0),
-                                          threads)
-            codec = {"value": round(cv, 3), "unit": "GB/s", "cores": cused,
-                     "library": "liblz4 %d LZ4_decompress_safe" % oracle.oracle_lib().codec_lz4_version()}
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(mean_ms, 5),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u8", "data": "synthetic",
-            "config": {"workload": "lz4 block batch decode, 1024 x 64 KiB chunks (64 MiB out)",
-                       "format": "lz4", "chunks": N_CHUNKS, "chunk_bytes": CHUNK,
-                       "compressed_bytes": in_bytes, "parallelism": "replicas x%d" % world,
+            "config": {"workload": WORKLOAD % n, "format": "lz4", "chunks": n,
+                       "chunk_bytes": CHUNK, "compressed_bytes": in_bytes,
+                       "parallelism": "replicas x%d" % world,
                        "l2": "flushed before every timed launch (256 MiB memset)"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
-                         "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "unit": "GB/s", "frac": round(achieved / peak, 5),
                          "traffic": traffic_per_launch(), "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": in_bytes + out_bytes},
             "e2e": {"value": round(e2e, 3), "unit": "GB/s",
-                    "h2d_bytes_per_step": int(batch.d_src.numel() + meta_dev.numel() * 8),
-                    "d2h_bytes_per_step": 16 * n},
+                    "h2d_bytes_per_step": int(in_bytes + 32 * n),
+                    "d2h_bytes_per_step": 16 * n,
+                    "api": "cudec_lz4_decompress_stream_ctx, pinned host chunks -> HBM, "
+                           "host clock around the synchronous call",
+                    "ms_per_step": round(e2e_ms, 4)},
+            "per_format": {
+                "lz4": {"value": round(value, 3), "ms_per_step": round(mean_ms, 5)},
+                "snappy": {"value": round(world * out_bytes / (s_ms * 1e-3) / 1e9, 3),
+                           "ms_per_step": round(s_ms, 5),
+                           "roofline_frac": round((s_in + out_bytes) / (s_ms * 1e-3) / 1e9 / peak, 5)},
+            },
             "gpu_launches": args.steps,
             "clocks": clocks.summary(),
         }
-        if cpu:
-            line["cpu_baseline"] = cpu
-            line["cpu_codec"] = codec
+        if world == 1 and args.cpu_seconds > 0:
+            import oracle
+            kind = "ref_lz4" if oracle.ref_twin_lib() is not None else "oracle_lz4"
+            threads = os.cpu_count() or 1
+            v, used, reps = cpu_sample(kind, comps, caps, args.cpu_seconds, threads)
+            line["cpu_baseline"] = {
+                "value": round(v, 3), "unit": "GB/s", "cores": used,
+                "kind": "reference" if kind == "ref_lz4" else "port",
+                "sample": "%d passes over the same %d x 64 KiB batch (~%.0f s); reference "
+                          "twin tests/lz4_twin.h on a std::thread pool" % (reps, n, args.cpu_seconds)}
+            cv, cused, _ = cpu_sample("codec_lz4", comps, caps, min(args.cpu_seconds, 5.0), threads)
+            line["cpu_codec"] = {"value": round(cv, 3), "unit": "GB/s", "cores": cused,
+                                 "library": "liblz4 %d LZ4_decompress_safe"
+                                            % oracle.oracle_lib().codec_lz4_version()}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -175,10 +175,20 @@ cudec_status decode(cudec_stream_ctx& ctx, const void* const* src, const size_t*
         unsigned char* ds = static_cast<unsigned char*>(ctx.d_src[b].p);
         unsigned char* dout = static_cast<unsigned char*>(ctx.d_out[b].p);
         uint64_t* pm = static_cast<uint64_t*>(ctx.p_meta[b].p);
+        // Sources laid out back to back (the usual packed batch) go up in one
+        // copy straight from the caller's memory: a DMA when it is pinned, a
+        // driver-staged copy otherwise; no host staging pass either way.
+        bool contiguous = true;
+        for (size_t j = 1; j < wn && contiguous; ++j) {
+            const size_t i = begin + j;
+            if (sizes[i] && static_cast<const unsigned char*>(src[i]) !=
+                                static_cast<const unsigned char*>(src[i - 1]) + sizes[i - 1])
+                contiguous = false;
+        }
         size_t so = 0, oo = 0;
         for (size_t j = 0; j < wn; ++j) {
             const size_t i = begin + j;
-            if (sizes[i]) std::memcpy(ps + so, src[i], sizes[i]);
+            if (sizes[i] && !contiguous) std::memcpy(ps + so, src[i], sizes[i]);
             pm[j] = reinterpret_cast<uint64_t>(ds + so);
             pm[wave + j] = sizes[i];
             pm[2 * wave + j] = host_out ? reinterpret_cast<uint64_t>(dout + oo)
@@ -187,7 +197,8 @@ cudec_status decode(cudec_stream_ctx& ctx, const void* const* src, const size_t*
             so += sizes[i];
             if (host_out) oo += caps[i];
         }
-        if (so && cudaMemcpyAsync(ds, ps, so, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+        const void* up = contiguous ? src[begin] : static_cast<const void*>(ps);
+        if (so && cudaMemcpyAsync(ds, up, so, cudaMemcpyHostToDevice, s) != cudaSuccess) {
             fail = CUDEC_ERR_CUDA;
             break;
         }
