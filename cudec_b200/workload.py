@@ -178,3 +178,73 @@ def lz4f_compress(data, block_size_id=4, independent=True, content_checksum=Fals
     if L.LZ4F_isError(n):
         raise RuntimeError("LZ4F_compressFrame failed")
     return out.raw[:n]
+
+
+_zstd = None
+
+
+def _zstdlib():
+    global _zstd
+    if _zstd is None:
+        _zstd = ctypes.CDLL("libzstd.so.1")
+        _zstd.ZSTD_createCCtx.restype = ctypes.c_void_p
+        _zstd.ZSTD_freeCCtx.argtypes = [ctypes.c_void_p]
+        _zstd.ZSTD_CCtx_setParameter.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        _zstd.ZSTD_CCtx_setParameter.restype = ctypes.c_size_t
+        _zstd.ZSTD_compress2.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                         ctypes.c_void_p, ctypes.c_size_t]
+        _zstd.ZSTD_compress2.restype = ctypes.c_size_t
+        _zstd.ZSTD_compressBound.argtypes = [ctypes.c_size_t]
+        _zstd.ZSTD_compressBound.restype = ctypes.c_size_t
+        _zstd.ZSTD_isError.argtypes = [ctypes.c_size_t]
+        _zstd.ZSTD_isError.restype = ctypes.c_uint
+        _zstd.ZSTD_decompress.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
+                                          ctypes.c_size_t]
+        _zstd.ZSTD_decompress.restype = ctypes.c_size_t
+    return _zstd
+
+
+# ZSTD_cParameter / ZSTD_cParameter values from zstd.h (stable API)
+_ZSTD_C_LEVEL = 100
+_ZSTD_C_WINDOWLOG = 101
+_ZSTD_C_CONTENTSIZE = 200
+_ZSTD_C_CHECKSUM = 201
+
+
+def zstd_version():
+    return _zstdlib().ZSTD_versionNumber()
+
+
+def zstd_compress(data, level=3, window_log=20, checksum=False):
+    """One Zstd frame via libzstd ZSTD_compress2 (content size always
+    written; window log and checksum flag as given)."""
+    Z = _zstdlib()
+    data = bytes(data)
+    cctx = Z.ZSTD_createCCtx()
+    try:
+        for p, v in ((_ZSTD_C_LEVEL, level), (_ZSTD_C_WINDOWLOG, window_log),
+                     (_ZSTD_C_CONTENTSIZE, 1), (_ZSTD_C_CHECKSUM, 1 if checksum else 0)):
+            if Z.ZSTD_isError(Z.ZSTD_CCtx_setParameter(cctx, p, v)):
+                raise RuntimeError("ZSTD_CCtx_setParameter(%d)" % p)
+        bound = Z.ZSTD_compressBound(len(data))
+        out = ctypes.create_string_buffer(bound)
+        n = Z.ZSTD_compress2(cctx, out, bound, data, len(data))
+        if Z.ZSTD_isError(n):
+            raise RuntimeError("ZSTD_compress2 failed")
+        return out.raw[:n]
+    finally:
+        Z.ZSTD_freeCCtx(cctx)
+
+
+def zstd_decompress_ref(frame, cap):
+    """libzstd ZSTD_decompress: bytes, or None when libzstd rejects."""
+    Z = _zstdlib()
+    out = ctypes.create_string_buffer(max(cap, 1))
+    n = Z.ZSTD_decompress(out, cap, bytes(frame), len(frame))
+    return None if Z.ZSTD_isError(n) else out.raw[:n]
+
+
+def zstd_params(copy_prob=0.5, rle_prob=0.1):
+    """Zstd content: the LZ content generator with back-references up to
+    1 MiB and 10 % of events a run of one repeated byte (mean 64)."""
+    return GenParams(copy_prob, 64, 1.1, 8.0, 16.0, 4, 255, 1 << 20, rle_prob, 64.0, 0)

@@ -54,6 +54,8 @@ def oracle_lib():
         "oracle_lz4_decode": (ctypes.c_int, _DEC),
         "oracle_snappy_decode": (ctypes.c_int, _DEC),
         "oracle_lz4f_decode": (ctypes.c_int, _DEC),
+        "oracle_zstd_decode": (ctypes.c_int, _DEC),
+        "oracle_xxh64": (ctypes.c_uint64, [_U8P, _U64, _U64]),
         "oracle_lz4_decode_batch": (ctypes.c_int, _BATCH),
         "oracle_snappy_decode_batch": (ctypes.c_int, _BATCH),
         "codec_decode_batch": (ctypes.c_int, [ctypes.c_int] + _BATCH),
@@ -70,6 +72,8 @@ def ref_twin_lib():
     return _load(REF_TWIN_LIB, {
         "ref_lz4_twin_decode": (ctypes.c_int, _DEC),
         "ref_snappy_twin_decode": (ctypes.c_int, _DEC),
+        "ref_zstd_twin_decode": (ctypes.c_int, _DEC),
+        "ref_zstd_twin_decode_batch": (ctypes.c_int, _BATCH),
         "ref_lz4_twin_decode_batch": (ctypes.c_int, _BATCH),
         "ref_snappy_twin_decode_batch": (ctypes.c_int, _BATCH),
     })
@@ -122,6 +126,17 @@ def ref_lz4f_decode(frame, cap):
     return st, out[:w.value].tobytes()
 
 
+def zstd_decode(frame, cap):
+    """(status, bytes) from the C restatement of the Zstd frame decode."""
+    return _decode_one(oracle_lib().oracle_zstd_decode, frame, cap)
+
+
+def ref_zstd_decode(frame, cap):
+    """(status, bytes) from the reference's twin driver, or None if unbuilt."""
+    h = ref_twin_lib()
+    return None if h is None else _decode_one(h.ref_zstd_twin_decode, frame, cap)
+
+
 def snappy_decode(comp, cap):
     return _decode_one(oracle_lib().oracle_snappy_decode, comp, cap)
 
@@ -172,7 +187,7 @@ class HostBatch:
 
 def decode_batch(kind, batch, threads):
     """Run a batch driver: kind in {"oracle_lz4", "oracle_snappy", "ref_lz4",
-    "ref_snappy", "codec_lz4", "codec_zstd"}. Returns the thread count used."""
+    "ref_snappy", "ref_zstd", "codec_lz4", "codec_zstd"}. Returns the thread count used."""
     if kind.startswith("oracle_"):
         fn = getattr(oracle_lib(), "oracle_%s_decode_batch" % kind[7:])
         return fn(*batch.args(), threads)

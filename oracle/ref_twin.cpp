@@ -9,11 +9,14 @@
 //   tests/lz4_twin.h:41-86      cudec_test::Lz4TwinDecode over src/lz4_block.h
 //   tests/snappy_twin.h:140-160 cudec_test::SnappyTwinDecode over
 //                               src/snappy_block.h
+//   tests/zstd_twin_driver.h:178-390 cudec_twin::DecodeFrame over
+//                               src/zstd_*.h
 //
 // The batch shims run those same functions over a std::thread pool; they are
 // the "reference CPU implementation" timed by `bench.py --impl reference`.
 #include "lz4_twin.h"
 #include "snappy_twin.h"
+#include "zstd_twin_driver.h"
 
 #include <atomic>
 #include <cstdint>
@@ -42,6 +45,17 @@ int ref_snappy_twin_decode(const uint8_t* src, uint64_t n, uint8_t* dst,
     if (st != CUDEC_OK) return st;
     if (!out.empty()) std::memcpy(dst, out.data(), out.size());
     *written = out.size();
+    return CUDEC_OK;
+}
+
+int ref_zstd_twin_decode(const uint8_t* src, uint64_t n, uint8_t* dst,
+                         uint64_t cap, uint64_t* written) {
+    cudec_twin::Bytes frame(src, src + n);
+    cudec_twin::Run run = cudec_twin::DecodeFrame(frame, cap);
+    *written = 0;
+    if (!run.ok) return run.status;
+    if (!run.output.empty()) std::memcpy(dst, run.output.data(), run.output.size());
+    *written = run.output.size();
     return CUDEC_OK;
 }
 
@@ -74,6 +88,14 @@ int ref_lz4_twin_decode_batch(const uint8_t* const* src, const uint64_t* sizes,
                               uint64_t n, int32_t* status, uint64_t* written,
                               int threads) {
     return ref_batch(ref_lz4_twin_decode, src, sizes, dst, caps, n, status,
+                     written, threads);
+}
+
+int ref_zstd_twin_decode_batch(const uint8_t* const* src, const uint64_t* sizes,
+                               uint8_t* const* dst, const uint64_t* caps,
+                               uint64_t n, int32_t* status, uint64_t* written,
+                               int threads) {
+    return ref_batch(ref_zstd_twin_decode, src, sizes, dst, caps, n, status,
                      written, threads);
 }
 

@@ -117,6 +117,34 @@ def snappy_vectors():
     return out
 
 
+def zstd_vectors():
+    """fuzz/corpus/fuzz_zstd_frame/* (the whole input is the frame,
+    fuzz/fuzz_zstd_frame.cpp) decoded whole with capacity 1 MiB, plus small
+    libzstd frames (levels 1/19, checksum on) kept as bytes so the vectors do
+    not depend on the compressor version; verdicts from the reference's twin
+    driver (tests/zstd_twin_driver.h)."""
+    out = []
+    d = os.path.join(REF, "fuzz", "corpus", "fuzz_zstd_frame")
+    cap = 1 << 20
+    for f in sorted(os.listdir(d)):
+        body = open(os.path.join(d, f), "rb").read()[: 1 << 14]
+        twin = oracle.ref_zstd_decode(body, cap)
+        got = workload.zstd_decompress_ref(body, cap)
+        out.append(_record("seed/" + f, "zstd", body, cap, twin, got is not None, got))
+    import numpy as np
+    buf, offs = workload.generate([3000, 20000], [workload.zstd_params(0.5, 0.1)],
+                                  seeds=np.array([11, 12], dtype=np.uint64))
+    for i, (o, n) in enumerate(zip(offs, [3000, 20000])):
+        raw = buf[int(o):int(o) + n].tobytes()
+        for lvl in (1, 19):
+            body = workload.zstd_compress(raw, lvl, 20, True)
+            twin = oracle.ref_zstd_decode(body, n)
+            got = workload.zstd_decompress_ref(body, n)
+            out.append(_record("libzstd/%d-L%d" % (n, lvl), "zstd", body, n, twin,
+                               got is not None, got))
+    return out
+
+
 def _declared(body):
     v = 0
     for k in range(5):
@@ -135,7 +163,8 @@ def main():
     if oracle.ref_twin_lib() is None:
         sys.exit("oracle/_ref/libref_twin.so missing: run make -f oracle/Makefile")
     for name, vecs in (("lz4_block.json", lz4_vectors()),
-                       ("snappy_block.json", snappy_vectors())):
+                       ("snappy_block.json", snappy_vectors()),
+                       ("zstd_frame.json", zstd_vectors())):
         with open(os.path.join(OUT, name), "w") as f:
             json.dump({"generated_by": "tests/golden/make_golden.py",
                        "lz4_version": workload.lz4_version(),
