@@ -23,7 +23,12 @@ the launch itself is bracketed by CUDA events on its stream.
             against the measured HBM copy bandwidth
   cpu_baseline  the reference's own host decoder (its twin, compiled from
             its sources) on all host cores, same chunks
-  per_format    the same measurement for raw Snappy (same content)
+  per_format    the same measurement for raw Snappy (same content) and for
+            Zstd: 4,096 frames of 1 MiB (1 MiB window, 128 KiB blocks, 10%
+            repeated-byte runs, back-references up to 1 MiB), libzstd level 3
+            and level 19 as two batches; `--zstd-unique` distinct frames are
+            compressed and laid out repeatedly so the batch fills 4 GiB of
+            output (every frame is its own copy in HBM; L2 flushed)
 
 `--impl reference` times that reference CPU decoder alone, same metric.
 Multi-GPU: replicas (chunks are independent; no exchange step).
@@ -60,7 +65,34 @@ def parse_args():
     ap.add_argument("--chunks", type=int, default=N_CHUNKS,
                     help="chunk count (the headline workload is 1024; smaller "
                          "counts are for profiler captures)")
+    ap.add_argument("--zstd-frames", type=int, default=4096,
+                    help="Zstd frames per batch (0 skips the Zstd legs)")
+    ap.add_argument("--zstd-unique", type=int, default=128,
+                    help="distinct Zstd frames compressed per level")
     return ap.parse_args()
+
+
+ZSTD_FRAME = 1 << 20
+
+
+def _zstd_job(job):
+    from cudec_b200 import workload as W
+    seed, level = job
+    buf, offs = W.generate([ZSTD_FRAME], [W.zstd_params(0.5, 0.1)],
+                           seeds=np.array([seed], dtype=np.uint64))
+    raw = buf[:ZSTD_FRAME].tobytes()
+    return raw, W.zstd_compress(raw, level, 20, False)
+
+
+def zstd_workload(unique, level):
+    """`unique` distinct 1 MiB frames at `level`, compressed in worker
+    processes (spawned, so no CUDA state is forked)."""
+    import multiprocessing as mp
+    from cudec_b200 import workload as W
+    jobs = [(W.chunk_seed(CONFIG_SEED, 3, i), level) for i in range(unique)]
+    with mp.get_context("spawn").Pool(min(os.cpu_count() or 1, 32)) as pool:
+        out = pool.map(_zstd_job, jobs)
+    return [o[0] for o in out], [o[1] for o in out]
 
 
 def workload(n, fmt="lz4"):
@@ -288,6 +320,33 @@ def main():
     s_in = sum(len(c) for c in scomps)
     del sbatch
 
+    # ---- Zstd, 1 MiB frames at levels 3 and 19 ------------------------
+    zstd_lines = {}
+    if args.zstd_frames > 0:
+        for level in (3, 19):
+            zraws, zuniq = zstd_workload(min(args.zstd_unique, args.zstd_frames), level)
+            zn = args.zstd_frames
+            zcomps = [zuniq[i % len(zuniq)] for i in range(zn)]
+            zbatch = DeviceBatch(zcomps, [ZSTD_FRAME] * zn, device=dev, poison=None)
+            z_ms = max_over_ranks(time_device(torch, zbatch, "zstd", stream, flush,
+                                              max(args.steps // 20, 3), warm))
+            zres = zbatch.results()
+            assert (zres["status"] == 0).all() and (zres["bytes_written"] == ZSTD_FRAME).all()
+            zdst = zbatch.dst_host() if zn <= 1024 else None
+            for i in range(0, zn, max(zn // 16, 1)):
+                got = zbatch.output(i, zdst, ZSTD_FRAME) if zdst is not None else \
+                    zbatch.d_dst[int(zbatch.dst_offs[i]):int(zbatch.dst_offs[i]) + ZSTD_FRAME].cpu().numpy().tobytes()
+                assert got == zraws[i % len(zraws)]
+            z_in = zbatch.src_bytes
+            z_out = ZSTD_FRAME * zn
+            zstd_lines["zstd_l%d" % level] = {
+                "value": round(world * z_out / (z_ms * 1e-3) / 1e9, 3),
+                "ms_per_step": round(z_ms, 4), "frames": zn, "unique_frames": len(zuniq),
+                "frame_bytes": ZSTD_FRAME, "compressed_bytes": z_in,
+                "roofline_frac": round((z_in + z_out) / (z_ms * 1e-3) / 1e9 / peaks()[0], 5)}
+            del zbatch
+            torch.cuda.empty_cache()
+
     # ---- end to end through the C ABI with host buffers ----------------
     # cudec_lz4_decompress_stream_ctx: compressed chunks in pinned host memory,
     # destinations in HBM; the synchronous call covers the host->device copy,
@@ -350,6 +409,7 @@ def main():
                 "snappy": {"value": round(world * out_bytes / (s_ms * 1e-3) / 1e9, 3),
                            "ms_per_step": round(s_ms, 5),
                            "roofline_frac": round((s_in + out_bytes) / (s_ms * 1e-3) / 1e9 / peak, 5)},
+                **zstd_lines,
             },
             "gpu_launches": args.steps,
             "clocks": clocks.summary(),

@@ -52,6 +52,8 @@ SIGNATURES = {
     "cudec_version": (ctypes.c_int, []),
     "cudec_lz4_decompress_batch": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P]),
     "cudec_snappy_decompress_batch": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P]),
+    "cudec_zstd_workspace_bytes": (ctypes.c_size_t, [_SZ]),
+    "cudec_zstd_decompress_batch": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P, _SZ, _P]),
     "cudec_lz4f_decompress": (ctypes.c_int, [_P, _SZ, _P, _SZ, _P]),
     "cudec_stream_ctx_create": (ctypes.c_int, [_P]),
     "cudec_lz4_decompress_stream_ctx": (ctypes.c_int, [_P, _P, _P, _P, _P, _SZ, ctypes.c_int, _P]),
@@ -100,6 +102,17 @@ def snappy_decompress_batch(d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_caps, n,
     """cudec_snappy_decompress_batch (same contract as the LZ4 entry)."""
     return _batch_call("cudec_snappy_decompress_batch", d_src_ptrs, d_src_sizes,
                        d_dst_ptrs, d_dst_caps, n, d_results, stream)
+
+
+def zstd_workspace_bytes(n):
+    return lib().cudec_zstd_workspace_bytes(n)
+
+
+def zstd_decompress_batch(d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_caps, n, d_results,
+                          d_workspace, workspace_bytes, stream=None):
+    """cudec_zstd_decompress_batch (one Zstd frame per chunk)."""
+    return lib().cudec_zstd_decompress_batch(d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_caps,
+                                             n, d_results, d_workspace, workspace_bytes, stream)
 
 
 BATCH_ENTRIES = {

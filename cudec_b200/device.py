@@ -75,7 +75,17 @@ class DeviceBatch:
         """Launch the format's batch entry on `stream` (torch stream or None =
         current stream). Returns the synchronous status."""
         s = (stream or torch.cuda.current_stream(self.device)).cuda_stream
+        if fmt == "zstd":
+            ws = self.workspace()
+            return cd.zstd_decompress_batch(*self.args(), ws.data_ptr(), ws.numel(), s)
         return cd.BATCH_ENTRIES[fmt](*self.args(), s)
+
+    def workspace(self):
+        """Device workspace for the Zstd entry (allocated once per batch)."""
+        if getattr(self, "_ws", None) is None:
+            self._ws = torch.empty(cd.zstd_workspace_bytes(self.n), dtype=torch.uint8,
+                                   device=self.device)
+        return self._ws
 
     def results(self):
         raw = self.d_results.cpu().numpy().tobytes()

@@ -114,6 +114,30 @@ cudec_status cudec_snappy_decompress_batch(const void* const* d_src_ptrs,
                                            cudec_chunk_result* d_results,
                                            cudec_stream_t stream);
 
+/* Zstd frames (RFC 8878), one frame per chunk, in the reference's v1 subset
+ * (docs/MASTERPLAN.md:1208-1251; ladder src/zstd_frame.h:196-409 and the
+ * units it drives, status mapping tests/zstd_twin_driver.h:178-390). Not
+ * shipped by the reference as a kernel; same contract shape as the LZ4 entry
+ * plus a caller-owned device workspace, so the call still allocates nothing.
+ * Statuses: skippable frames, a dictionary id, no content size, a window above
+ * 8 MB -> CUDEC_ERR_UNSUPPORTED; content size above the capacity or output
+ * past it -> CUDEC_ERR_OUTPUT_TOO_SMALL; any other inconsistency (headers,
+ * literals, tables, sequences, repeat offsets, window, content size,
+ * checksum, trailing bytes) -> CUDEC_ERR_CORRUPT_INPUT. d_workspace must hold
+ * cudec_zstd_workspace_bytes(chunk_count) bytes (a NULL or short workspace is
+ * CUDEC_ERR_INVALID_ARGUMENT); it may be reused once the launch completes. */
+size_t cudec_zstd_workspace_bytes(size_t chunk_count);
+
+cudec_status cudec_zstd_decompress_batch(const void* const* d_src_ptrs,
+                                         const size_t* d_src_sizes,
+                                         void* const* d_dst_ptrs,
+                                         const size_t* d_dst_capacities,
+                                         size_t chunk_count,
+                                         cudec_chunk_result* d_results,
+                                         void* d_workspace,
+                                         size_t workspace_bytes,
+                                         cudec_stream_t stream);
+
 /* ---------------------------------------------------------------------
  * LZ4 frame (.lz4 container), host memory in and out, synchronous.
  * Replaces: include/cudec.h:130-132, src/frame.cpp:401-422.

@@ -94,3 +94,17 @@ def test_c99_consumer_compiles_and_links(tmp_path):
                    check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True)
     assert out.returncode == 0 and out.stdout.strip() == "ok", (out.returncode, out.stderr)
+
+
+def test_zstd_workspace_rejects_synchronously():
+    buf, a = _fake()
+    ws = cd.zstd_workspace_bytes(4)
+    assert ws == 4 * 128 * 1024
+    assert cd.zstd_workspace_bytes(1) == ws  # rounded up to a CTA's warps
+    assert cd.zstd_workspace_bytes(1 << 20) == cd.zstd_workspace_bytes(4096)
+    z = cd.zstd_decompress_batch
+    assert z(a, a, a, a, 4, a, None, ws, None) == cd.ERR_INVALID_ARGUMENT
+    assert z(a, a, a, a, 4, a, a, ws - 1, None) == cd.ERR_INVALID_ARGUMENT
+    assert z(None, a, a, a, 4, a, a, ws, None) == cd.ERR_INVALID_ARGUMENT
+    assert z(a, a, a, a, 0, a, a, ws, None) == cd.ERR_INVALID_ARGUMENT
+    assert z(a, a, a, a, 4, a + 8, a, ws, None) == cd.ERR_INVALID_ARGUMENT
