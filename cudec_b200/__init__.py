@@ -54,6 +54,7 @@ SIGNATURES = {
     "cudec_snappy_decompress_batch": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P]),
     "cudec_zstd_workspace_bytes": (ctypes.c_size_t, [_SZ]),
     "cudec_zstd_decompress_batch": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P, _SZ, _P]),
+    "cudec_zstd_decompress_batch_noalloc": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P]),
     "cudec_lz4f_decompress": (ctypes.c_int, [_P, _SZ, _P, _SZ, _P]),
     "cudec_stream_ctx_create": (ctypes.c_int, [_P]),
     "cudec_lz4_decompress_stream_ctx": (ctypes.c_int, [_P, _P, _P, _P, _P, _SZ, ctypes.c_int, _P]),
@@ -113,6 +114,16 @@ def zstd_decompress_batch(d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_caps, n, d_
     """cudec_zstd_decompress_batch (one Zstd frame per chunk)."""
     return lib().cudec_zstd_decompress_batch(d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_caps,
                                              n, d_results, d_workspace, workspace_bytes, stream)
+
+
+ZSTD_NOALLOC_MAX_CHUNKS = 64
+
+
+def zstd_decompress_batch_noalloc(d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_caps, n,
+                                  d_results, stream=None):
+    """cudec_zstd_decompress_batch_noalloc (library-owned scratch, <= 64 chunks)."""
+    return lib().cudec_zstd_decompress_batch_noalloc(d_src_ptrs, d_src_sizes, d_dst_ptrs,
+                                                     d_dst_caps, n, d_results, stream)
 
 
 BATCH_ENTRIES = {

@@ -465,3 +465,69 @@ cudec_status cudec_zstd_decompress_batch(const void* const* d_src_ptrs,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant: the same kernel, its literal slots taken from a
+// file-scope device array instead of a caller workspace. One slot per frame,
+// so a call takes at most kNoAllocChunks frames (8 MiB of slots). The array's
+// address is looked up once per device. Nothing in it needs to start at zero:
+// every literal byte a sequence reads was written by the same frame's
+// Huffman decode first. Calls whose launches overlap in time on one device
+// share the array and race; calls queued on one stream are ordered.
+namespace cdb {
+namespace zstd {
+
+constexpr size_t kNoAllocChunks = CUDEC_ZSTD_NOALLOC_MAX_CHUNKS;
+constexpr int kNoAllocMaxDevices = 256;
+static_assert(kNoAllocChunks % kWarpsPerCta == 0, "whole CTAs of slots");
+
+static __device__ __align__(256) uint8_t g_noalloc_slots[kNoAllocChunks * kLitSlot];
+
+static std::atomic<uint8_t*> g_noalloc_addr[kNoAllocMaxDevices];
+
+// Device address of the slot array on the current device (nullptr on error).
+static uint8_t* noalloc_slots(cudaError_t* err) {
+    int dev = 0;
+    *err = cudaGetDevice(&dev);
+    if (*err != cudaSuccess) return nullptr;
+    if (dev < 0 || dev >= kNoAllocMaxDevices) {
+        *err = cudaErrorInvalidDevice;
+        return nullptr;
+    }
+    uint8_t* p = g_noalloc_addr[dev].load(std::memory_order_acquire);
+    if (p != nullptr) return p;
+    void* a = nullptr;
+    *err = cudaGetSymbolAddress(&a, g_noalloc_slots);
+    if (*err != cudaSuccess || a == nullptr) {
+        if (*err == cudaSuccess) *err = cudaErrorInvalidSymbol;
+        return nullptr;
+    }
+    g_noalloc_addr[dev].store(static_cast<uint8_t*>(a), std::memory_order_release);
+    return static_cast<uint8_t*>(a);
+}
+
+}  // namespace zstd
+}  // namespace cdb
+
+extern "C" cudec_status cudec_zstd_decompress_batch_noalloc(
+    const void* const* d_src_ptrs, const size_t* d_src_sizes, void* const* d_dst_ptrs,
+    const size_t* d_dst_capacities, size_t chunk_count, cudec_chunk_result* d_results,
+    cudec_stream_t stream) {
+    const cudec_status v = cdb::validate_batch(d_src_ptrs, d_src_sizes, d_dst_ptrs,
+                                               d_dst_capacities, chunk_count, d_results);
+    if (v != CUDEC_OK) return v;
+    if (chunk_count > cdb::zstd::kNoAllocChunks) return CUDEC_ERR_INVALID_ARGUMENT;
+    (void)cudaGetLastError();
+    cudaError_t err = cudaSuccess;
+    uint8_t* slots = cdb::zstd::noalloc_slots(&err);
+    if (slots == nullptr) {
+        (void)cudaGetLastError();
+        return CUDEC_ERR_CUDA;
+    }
+    const unsigned grid = static_cast<unsigned>(
+        (chunk_count + cdb::zstd::kWarpsPerCta - 1) / cdb::zstd::kWarpsPerCta);
+    cdb::zstd::zstd_decode_kernel<<<grid, cdb::zstd::kCtaThreads, 0,
+                                    reinterpret_cast<cudaStream_t>(stream)>>>(
+        d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_capacities, chunk_count, d_results, slots);
+    return cudaGetLastError() == cudaSuccess ? CUDEC_OK : CUDEC_ERR_CUDA;
+}

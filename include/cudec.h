@@ -138,6 +138,25 @@ cudec_status cudec_zstd_decompress_batch(const void* const* d_src_ptrs,
                                          size_t workspace_bytes,
                                          cudec_stream_t stream);
 
+/* Allocation-free Zstd batch entry, for callers that cannot allocate device
+ * memory. No counterpart in the reference. Same statuses and records as
+ * cudec_zstd_decompress_batch, but the per-frame literal slots come from a
+ * static device array inside the library (8 MiB), so a call takes at most
+ * CUDEC_ZSTD_NOALLOC_MAX_CHUNKS chunks: a larger chunk_count is
+ * CUDEC_ERR_INVALID_ARGUMENT, returned before any CUDA call. The array is
+ * shared by every call on a device: calls whose launches overlap in time
+ * (different streams or host threads) race on it; calls queued on one stream
+ * are ordered and safe. */
+#define CUDEC_ZSTD_NOALLOC_MAX_CHUNKS 64
+
+cudec_status cudec_zstd_decompress_batch_noalloc(const void* const* d_src_ptrs,
+                                                 const size_t* d_src_sizes,
+                                                 void* const* d_dst_ptrs,
+                                                 const size_t* d_dst_capacities,
+                                                 size_t chunk_count,
+                                                 cudec_chunk_result* d_results,
+                                                 cudec_stream_t stream);
+
 /* ---------------------------------------------------------------------
  * LZ4 frame (.lz4 container), host memory in and out, synchronous.
  * Replaces: include/cudec.h:130-132, src/frame.cpp:401-422.
