@@ -12,7 +12,7 @@
 
 #include "cudec.h"
 #include "launch.h"
-#include "lz_block_kernel.cuh"
+#include "lz_warp_kernel.cuh"
 
 namespace cdb {
 
@@ -30,22 +30,32 @@ cudec_status validate_batch(const void* const* src, const size_t* src_sizes,
 
 namespace {
 
-// Per-device one-time setup: the kernels need more than 48 KB of dynamic
-// shared memory, which must be opted into once per device and kernel.
+// Per-device one-time setup: the kernels use more than 48 KB of dynamic
+// shared memory (opted into once per device and kernel), and the persistent
+// grid is at most the resident CTAs per SM times the SM count.
 constexpr int kMaxDevices = 64;
 std::atomic<int> g_lz4_ready[kMaxDevices];
 std::atomic<int> g_snappy_ready[kMaxDevices];
 std::atomic<int> g_sm_count[kMaxDevices];
 
 template <class Fmt>
-cudaError_t prepare(std::atomic<int>* ready, int dev) {
+cudaError_t prepare(std::atomic<int>* ready, int dev, int* per_sm) {
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    if (ready[dev].load(std::memory_order_acquire)) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(lz_decode_kernel<Fmt>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(kLzSmemBytes));
+    int v = ready[dev].load(std::memory_order_acquire);
+    if (v > 0) {
+        *per_sm = v;
+        return cudaSuccess;
+    }
+    constexpr int kSmem = static_cast<int>(lzw::kWarps * lzw::kWarpSmem);
+    cudaError_t e = cudaFuncSetAttribute(lzw::lz_warp_kernel<Fmt>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
     if (e != cudaSuccess) return e;
-    ready[dev].store(1, std::memory_order_release);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, lzw::lz_warp_kernel<Fmt>,
+                                                      lzw::kThreads, kSmem);
+    if (e != cudaSuccess) return e;
+    if (v <= 0) return cudaErrorInvalidConfiguration;
+    ready[dev].store(v, std::memory_order_release);
+    *per_sm = v;
     return cudaSuccess;
 }
 
@@ -72,12 +82,14 @@ static cudec_status launch_lz(std::atomic<int>* ready, const void* const* src,
     (void)cudaGetLastError();
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return CUDEC_ERR_CUDA;
-    if (prepare<Fmt>(ready, dev) != cudaSuccess) return CUDEC_ERR_CUDA;
+    int per_sm = 0;
+    if (prepare<Fmt>(ready, dev, &per_sm) != cudaSuccess) return CUDEC_ERR_CUDA;
     const int sms = device_sm_count(dev);
     if (sms <= 0) return CUDEC_ERR_CUDA;
-    const size_t max_blocks = static_cast<size_t>(sms) * 2;
-    const unsigned grid = static_cast<unsigned>(n < max_blocks ? n : max_blocks);
-    lz_decode_kernel<Fmt><<<grid, kThreads, kLzSmemBytes, stream>>>(
+    const size_t max_blocks = static_cast<size_t>(sms) * per_sm;
+    const size_t want = (n + lzw::kWarps - 1) / lzw::kWarps;
+    const unsigned grid = static_cast<unsigned>(want < max_blocks ? want : max_blocks);
+    lzw::lz_warp_kernel<Fmt><<<grid, lzw::kThreads, lzw::kWarps * lzw::kWarpSmem, stream>>>(
         src, src_sizes, dst, caps, n, results);
     return cudaGetLastError() == cudaSuccess ? CUDEC_OK : CUDEC_ERR_CUDA;
 }
@@ -93,7 +105,7 @@ cudec_status cudec_lz4_decompress_batch(const void* const* d_src_ptrs,
                                         size_t chunk_count,
                                         cudec_chunk_result* d_results,
                                         cudec_stream_t stream) {
-    return cdb::launch_lz<cdb::Lz4Format>(
+    return cdb::launch_lz<cdb::lzw::Lz4>(
         cdb::g_lz4_ready, d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_capacities,
         chunk_count, d_results, reinterpret_cast<cudaStream_t>(stream));
 }
@@ -105,7 +117,7 @@ cudec_status cudec_snappy_decompress_batch(const void* const* d_src_ptrs,
                                            size_t chunk_count,
                                            cudec_chunk_result* d_results,
                                            cudec_stream_t stream) {
-    return cdb::launch_lz<cdb::SnappyFormat>(
+    return cdb::launch_lz<cdb::lzw::Snappy>(
         cdb::g_snappy_ready, d_src_ptrs, d_src_sizes, d_dst_ptrs,
         d_dst_capacities, chunk_count, d_results,
         reinterpret_cast<cudaStream_t>(stream));

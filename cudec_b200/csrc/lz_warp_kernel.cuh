@@ -1,0 +1,892 @@
+// Warp-per-chunk decoder for the byte-oriented LZ formats (LZ4 block, raw
+// Snappy).
+//
+// One warp owns one chunk at a time (persistent grid-stride over the batch).
+// The chunk's compressed bytes stream through a per-warp shared-memory input
+// window (kIn bytes, filled ahead of the parse by cp.async). For each parse
+// window of kPW input positions starting at a known token:
+//
+//   1. every lane evaluates the format's speculative `step` for its share of
+//      the positions ("where would the next token start if one started
+//      here"), and four doubling rounds turn that table into 2-, 4-, 8- and
+//      16-hop tables, so lane l finds the l-th following token in five
+//      lookups: the true token chain, 32 tokens at a time, with no serial
+//      walk;
+//   2. each lane runs the format's exact accept/reject ladder on its token
+//      (output position from a warp scan of the token lengths); the first
+//      failing or terminal token decides the chunk exactly as the serial
+//      parser would;
+//   3. tokens of at most kBig bytes execute lane-parallel through a per-warp
+//      output ring (kRing bytes, indexed by destination address mod kRing,
+//      so ring blocks and destination blocks share alignment): literal runs
+//      first, then matches in frontier rounds (a lane copies once every byte
+//      its source reads lies below the lowest unfinished match start; short
+//      periods are replicated in registers); completed 16-byte blocks leave
+//      the ring as aligned, coalesced 16-byte stores. Match sources older
+//      than the ring are read back from the destination. Longer tokens are
+//      copied by the whole warp straight to the destination.
+//
+// Statuses follow the reference ladders exactly: LZ4 iderex/cudec
+// src/lz4_block.h:95-258, Snappy src/snappy_block.h:172-435.
+#pragma once
+
+#include <cstdint>
+
+#include "cudec.h"
+
+namespace cdb {
+namespace lzw {
+
+constexpr uint32_t kWarps = 4;               // warps per CTA
+constexpr uint32_t kThreads = 32 * kWarps;
+constexpr uint32_t kRing = 8192;             // output ring per warp (bytes)
+constexpr uint32_t kIn = 4096;               // input window per warp (bytes)
+constexpr uint32_t kInAhead = kIn - 64;      // fill up to this far past the parse
+constexpr uint32_t kBatchMax = 4096;         // output bytes staged per batch
+constexpr uint64_t kBig = 256;               // longer tokens are copied by the whole warp
+constexpr uint32_t kPW = 1024;               // parse window (token positions per table)
+constexpr uint32_t kLevels = 5;              // hop tables: 1, 2, 4, 8, 16 tokens
+constexpr uint32_t kExit = 0xFFFF;           // hop leaves the window
+constexpr uint32_t kWarpSmem = kRing + kIn + kLevels * kPW * 2;
+constexpr unsigned kFull = 0xffffffffu;
+constexpr uint64_t kNone = ~0ull;            // no next token (speculative step)
+static_assert(kBatchMax + 16 <= kRing, "a batch never overwrites unflushed bytes");
+
+// Profiling builds (-DCDB_PHASE_TIMING) accumulate per-phase SM cycles and
+// event counts over all chunks of a launch.
+#ifdef CDB_PHASE_TIMING
+__device__ unsigned long long lzw_cycles[8];
+__device__ unsigned long long lzw_events[8];
+#define LZW_T(v) const long long v = clock64()
+#define LZW_ADD(i, t0) \
+    if (lane == 0) atomicAdd(&lzw_cycles[i], static_cast<unsigned long long>(clock64() - (t0)))
+#define LZW_EV(i, n) \
+    if (lane == 0) atomicAdd(&lzw_events[i], static_cast<unsigned long long>(n))
+#else
+#define LZW_T(v)
+#define LZW_ADD(i, t0)
+#define LZW_EV(i, n)
+#endif
+
+// One parsed sequence: lit literal bytes from input offset lit_src, then ml
+// bytes copied from off bytes back; next = the following token's position;
+// done = the chunk ends after this sequence (LZ4's terminal literal run).
+struct Seq {
+    uint64_t lit_src, lit, ml, next;
+    uint32_t off;
+    bool done;
+};
+
+__device__ __forceinline__ uint32_t ldb(const uint8_t* g, uint64_t p) {
+    return __ldg(g + p);
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// The chunk's compressed bytes: positions in [lo, lo + span) come from the
+// shared-memory window (indexed by global address mod kIn, so its 16-byte
+// blocks are the input's aligned blocks), others straight from global. A
+// refill in flight only writes slots of positions below lo.
+struct In {
+    const uint8_t* g;
+    const uint8_t* win;
+    uintptr_t gbase;
+    uint64_t lo, span;  // the window holds positions [lo, lo + span)
+    __device__ __forceinline__ bool held(uint64_t q, uint64_t m) const {
+        return q >= lo && q - lo + m <= span;
+    }
+    __device__ __forceinline__ uint32_t at(uint64_t q) const {
+        if (q - lo < span)
+            return win[(static_cast<uint32_t>(gbase) + static_cast<uint32_t>(q)) & (kIn - 1)];
+        return ldb(g, q);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// LZ4 block (src/lz4_block.h:139-258 Lz4Parser::Next, :95-128
+// AccumulateLength; constants :46-66).
+struct Lz4 {
+    static constexpr uint64_t kMfLimit = 12;
+    static constexpr uint64_t kSrcSlack = 8;
+    static constexpr uint64_t kLastLiterals = 5;
+
+    __device__ static int begin(const uint8_t*, uint64_t, uint64_t cap, uint64_t* first,
+                                uint64_t* limit) {
+        *first = 0;
+        *limit = cap;
+        return CUDEC_OK;
+    }
+    __device__ __forceinline__ static bool at_end(uint64_t, uint64_t) { return false; }
+    __device__ __forceinline__ static int finish(uint64_t, uint64_t) { return CUDEC_OK; }
+
+    __device__ __forceinline__ static int extend(const In& in, uint64_t S, uint64_t* q,
+                                                 uint64_t* len, uint64_t room, uint64_t margin,
+                                                 bool pre) {
+        if (pre && *q + margin >= S) return CUDEC_ERR_CORRUPT_INPUT;
+        uint32_t b;
+        do {
+            if (*q >= S) return CUDEC_ERR_CORRUPT_INPUT;
+            if (*len > room) return CUDEC_ERR_OUTPUT_TOO_SMALL;
+            b = in.at((*q)++);
+            *len += b;
+            if (*q + margin > S) return CUDEC_ERR_CORRUPT_INPUT;
+        } while (b == 255);
+        return CUDEC_OK;
+    }
+
+    // Speculative: where the next token starts if one starts at p (p < S),
+    // or kNone. No capacity checks; equals the exact ladder's next position
+    // for every token the ladder accepts as non-terminal.
+    __device__ __forceinline__ static uint64_t step(const In& in, uint64_t S, uint64_t p) {
+        const uint32_t tok = in.at(p);
+        uint64_t q = p + 1;
+        uint64_t lit = tok >> 4;
+        if (lit == 15) {
+            uint32_t b;
+            do {
+                if (q >= S) return kNone;
+                b = in.at(q++);
+                lit += b;
+            } while (b == 255);
+        }
+        if (lit > S - q) return kNone;
+        q += lit;
+        if (S - q < kSrcSlack) return kNone;
+        q += 2;
+        if ((tok & 15) == 15) {
+            uint32_t b;
+            do {
+                if (q >= S) return kNone;
+                b = in.at(q++);
+            } while (b == 255);
+        }
+        return q;
+    }
+
+    // Literal + match length of the token at p, unchecked (equal to the exact
+    // ladder's lengths for every token it accepts as non-terminal).
+    __device__ __forceinline__ static uint64_t length(const In& in, uint64_t S, uint64_t p) {
+        if (p >= S) return 0;
+        const uint32_t tok = in.at(p);
+        uint64_t q = p + 1;
+        uint64_t lit = tok >> 4;
+        if (lit == 15) {
+            uint32_t b;
+            do {
+                if (q >= S) return lit;
+                b = in.at(q++);
+                lit += b;
+            } while (b == 255);
+        }
+        uint64_t ml = (tok & 15) + 4;
+        if ((tok & 15) == 15) {
+            if (lit > S - q) return lit + ml;
+            q += lit + 2;
+            uint32_t b;
+            do {
+                if (q >= S) break;
+                b = in.at(q++);
+                ml += b;
+            } while (b == 255);
+        }
+        return lit + ml;
+    }
+
+    // The token at p with d bytes already produced; cap is the capacity.
+    __device__ __forceinline__ static int parse(const In& in, uint64_t S, uint64_t cap,
+                                                uint64_t p, uint64_t d, Seq* s) {
+        if (p >= S) return CUDEC_ERR_CORRUPT_INPUT;
+        const uint32_t tok = in.at(p);
+        uint64_t q = p + 1;
+        uint64_t lit = tok >> 4;
+        if (lit == 15) {
+            const int st = extend(in, S, &q, &lit, cap - d, 15, true);
+            if (st != CUDEC_OK) return st;
+        }
+        if (lit > S - q) return CUDEC_ERR_CORRUPT_INPUT;
+        if (lit > cap - d) return CUDEC_ERR_OUTPUT_TOO_SMALL;
+        s->lit_src = q;
+        s->lit = lit;
+        if (cap - d - lit < kMfLimit || S - q - lit < kSrcSlack) {
+            if (q + lit != S) return CUDEC_ERR_CORRUPT_INPUT;
+            // Capacity zero accepts only the single byte 0x00 (lz4_block.h:178-187).
+            if (cap == 0 && tok != 0) return CUDEC_ERR_CORRUPT_INPUT;
+            s->ml = 0;
+            s->off = 0;
+            s->next = S;
+            s->done = true;
+            return CUDEC_OK;
+        }
+        q += lit;
+        d += lit;
+        const uint32_t off = in.at(q) | (in.at(q + 1) << 8);
+        q += 2;
+        if (off == 0) return CUDEC_ERR_CORRUPT_INPUT;  // stricter than liblz4
+        if (off > d) return CUDEC_ERR_CORRUPT_INPUT;
+        uint64_t ml = (tok & 15) + 4;
+        if ((tok & 15) == 15) {
+            const int st = extend(in, S, &q, &ml, cap - d, 4, false);
+            if (st != CUDEC_OK) return st;
+        }
+        if (ml > cap - d) return CUDEC_ERR_OUTPUT_TOO_SMALL;
+        if (ml > cap - d - kLastLiterals) return CUDEC_ERR_CORRUPT_INPUT;
+        s->ml = ml;
+        s->off = off;
+        s->next = q;
+        s->done = false;
+        return CUDEC_OK;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Raw Snappy (src/snappy_block.h:172-223 SnappyDeclaredLength, :249-435
+// SnappyParser::Begin/Next). One element (literal OR copy) per Seq.
+struct Snappy {
+    __device__ static int begin(const uint8_t* g, uint64_t S, uint64_t cap, uint64_t* first,
+                                uint64_t* limit) {
+        uint64_t v = 0;
+        for (uint64_t k = 0; k < 5; ++k) {
+            if (k >= S) return CUDEC_ERR_CORRUPT_INPUT;
+            const uint32_t b = ldb(g, k);
+            if (k == 4 && b >= 16) return CUDEC_ERR_CORRUPT_INPUT;
+            v |= static_cast<uint64_t>(b & 0x7f) << (7 * k);
+            if (!(b & 0x80)) {
+                if (v > cap) return CUDEC_ERR_OUTPUT_TOO_SMALL;
+                *first = k + 1;
+                *limit = v;
+                return CUDEC_OK;
+            }
+        }
+        return CUDEC_ERR_CORRUPT_INPUT;
+    }
+    __device__ __forceinline__ static bool at_end(uint64_t p, uint64_t S) { return p == S; }
+    // Elements exhausted: success only at exact production of the declared length.
+    __device__ __forceinline__ static int finish(uint64_t d, uint64_t declared) {
+        return d == declared ? CUDEC_OK : CUDEC_ERR_CORRUPT_INPUT;
+    }
+
+    // Speculative next element position if one starts at p (p < S), or kNone.
+    __device__ __forceinline__ static uint64_t step(const In& in, uint64_t S, uint64_t p) {
+        const uint32_t tag = in.at(p);
+        const uint32_t kind = tag & 3;
+        if (kind == 0) {
+            const uint32_t l6 = tag >> 2;
+            uint64_t hdr = 1, len = l6;
+            if (l6 >= 60) {
+                const uint32_t extra = l6 - 59;
+                hdr += extra;
+                if (hdr > S - p) return kNone;
+                len = 0;
+                for (uint32_t i = 0; i < extra; ++i)
+                    len |= static_cast<uint64_t>(in.at(p + 1 + i)) << (8 * i);
+            }
+            len += 1;
+            const uint64_t q = p + hdr;
+            if (len > S - q) return kNone;
+            return q + len;
+        }
+        const uint64_t hdr = kind == 1 ? 2 : (kind == 2 ? 3 : 5);
+        if (hdr > S - p) return kNone;
+        return p + hdr;
+    }
+
+    __device__ __forceinline__ static uint64_t length(const In& in, uint64_t S, uint64_t p) {
+        if (p >= S) return 0;
+        const uint32_t tag = in.at(p);
+        const uint32_t kind = tag & 3;
+        if (kind == 0) {
+            const uint32_t l6 = tag >> 2;
+            if (l6 < 60) return l6 + 1;
+            const uint32_t extra = l6 - 59;
+            uint64_t len = 0;
+            for (uint32_t i = 0; i < extra && p + 1 + i < S; ++i)
+                len |= static_cast<uint64_t>(in.at(p + 1 + i)) << (8 * i);
+            return len + 1;
+        }
+        return kind == 1 ? 4 + ((tag >> 2) & 7) : (tag >> 2) + 1;
+    }
+
+    __device__ __forceinline__ static int parse(const In& in, uint64_t S,
+                                                uint64_t declared, uint64_t p, uint64_t d,
+                                                Seq* s) {
+        const uint32_t tag = in.at(p);
+        const uint32_t kind = tag & 3;
+        s->done = false;
+        if (kind == 0) {
+            const uint32_t l6 = tag >> 2;
+            uint64_t hdr = 1, len = l6;
+            if (l6 >= 60) {
+                const uint32_t extra = l6 - 59;
+                hdr += extra;
+                if (hdr > S - p) return CUDEC_ERR_CORRUPT_INPUT;
+                len = 0;
+                for (uint32_t i = 0; i < extra; ++i)
+                    len |= static_cast<uint64_t>(in.at(p + 1 + i)) << (8 * i);
+            }
+            len += 1;  // 64-bit: the 0xFFFFFFFF spelling is refused, not wrapped
+            const uint64_t q = p + hdr;
+            if (len > S - q) return CUDEC_ERR_CORRUPT_INPUT;
+            if (len > declared - d) return CUDEC_ERR_CORRUPT_INPUT;
+            s->lit_src = q;
+            s->lit = len;
+            s->ml = 0;
+            s->off = 0;
+            s->next = q + len;
+            return CUDEC_OK;
+        }
+        const uint32_t ob = kind == 1 ? 1 : (kind == 2 ? 2 : 4);
+        if (1 + ob > S - p) return CUDEC_ERR_CORRUPT_INPUT;
+        uint64_t off = 0, len;
+        for (uint32_t i = 0; i < ob; ++i) off |= static_cast<uint64_t>(in.at(p + 1 + i)) << (8 * i);
+        if (kind == 1) {
+            off |= static_cast<uint64_t>(tag >> 5) << 8;
+            len = 4 + ((tag >> 2) & 7);
+        } else {
+            len = (tag >> 2) + 1;
+        }
+        if (off == 0) return CUDEC_ERR_CORRUPT_INPUT;
+        if (off > d) return CUDEC_ERR_CORRUPT_INPUT;
+        if (len > declared - d) return CUDEC_ERR_CORRUPT_INPUT;
+        s->lit_src = p;
+        s->lit = 0;
+        s->ml = len;
+        s->off = static_cast<uint32_t>(off);
+        s->next = p + 1 + ob;
+        return CUDEC_OK;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// 16-byte windows. A window is 4 little-endian words holding bytes
+// [a, a + 16); only the first m are meaningful.
+
+// Bytes [mis, mis + 16) of the 32-byte pair (lo, hi).
+__device__ __forceinline__ uint4 shift32(uint4 lo, uint4 hi, uint32_t mis) {
+    const uint32_t k = mis >> 2, r = (mis & 3) * 8;
+    uint32_t w0, w1, w2, w3, w4;
+    if (k == 0) {
+        w0 = lo.x; w1 = lo.y; w2 = lo.z; w3 = lo.w; w4 = hi.x;
+    } else if (k == 1) {
+        w0 = lo.y; w1 = lo.z; w2 = lo.w; w3 = hi.x; w4 = hi.y;
+    } else if (k == 2) {
+        w0 = lo.z; w1 = lo.w; w2 = hi.x; w3 = hi.y; w4 = hi.z;
+    } else {
+        w0 = lo.w; w1 = hi.x; w2 = hi.y; w3 = hi.z; w4 = hi.w;
+    }
+    return make_uint4(__funnelshift_r(w0, w1, r), __funnelshift_r(w1, w2, r),
+                      __funnelshift_r(w2, w3, r), __funnelshift_r(w3, w4, r));
+}
+
+// m (1..16) input bytes at p (read-only for the kernel). The second aligned
+// block is read only when the m bytes reach into it, so no load touches an
+// aligned block without a requested byte in it.
+__device__ __forceinline__ uint4 ld16_input(const uint8_t* p, uint32_t m) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const uint32_t mis = a & 15;
+    const uint4* b = reinterpret_cast<const uint4*>(a - mis);
+    const uint4 lo = __ldg(b);
+    const uint4 hi = mis + m > 16 ? __ldg(b + 1) : make_uint4(0, 0, 0, 0);
+    return shift32(lo, hi, mis);
+}
+
+// m output bytes at p, written earlier by this warp (coherent loads).
+__device__ __forceinline__ uint4 ld16_output(const uint8_t* p, uint32_t m) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const uint32_t mis = a & 15;
+    const uint4* b = reinterpret_cast<const uint4*>(a - mis);
+    const uint4 lo = b[0];
+    const uint4 hi = mis + m > 16 ? b[1] : make_uint4(0, 0, 0, 0);
+    return shift32(lo, hi, mis);
+}
+
+__device__ __forceinline__ uint32_t byte_of(const uint4& v, uint32_t k) {
+    const uint32_t w = k < 4 ? v.x : k < 8 ? v.y : k < 12 ? v.z : v.w;
+    return (w >> ((k & 3) * 8)) & 0xff;
+}
+
+// Per-warp output state. Positions are byte offsets into the chunk's output.
+struct Out {
+    uint8_t* ring;     // kRing bytes of shared memory
+    uint8_t* dst;      // destination
+    uintptr_t dbase;   // destination address (ring index = (dbase + pos) mod kRing)
+    uint64_t vlo;      // positions >= vlo are held by the ring
+    uint64_t flushed;  // positions < flushed are in the destination
+
+    __device__ __forceinline__ uint32_t idx(uint64_t pos) const {
+        return static_cast<uint32_t>((dbase + pos) & (kRing - 1));
+    }
+
+    __device__ __forceinline__ uint4 ring16(uint64_t a) const {
+        const uint32_t ia = idx(a);
+        const uint32_t b0 = ia & ~15u, b1 = (b0 + 16) & (kRing - 1);
+        const uint4 lo = *reinterpret_cast<const uint4*>(ring + b0);
+        const uint4 hi = *reinterpret_cast<const uint4*>(ring + b1);
+        return shift32(lo, hi, ia & 15);
+    }
+
+    // m (1..16) already-written output bytes at position a.
+    __device__ __forceinline__ uint4 fetch16(uint64_t a, uint32_t m) const {
+        if (a >= vlo) return ring16(a);
+        if (a + m <= vlo) return ld16_output(dst + a, m);
+        uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (uint32_t j = 0; j < 16; ++j) {
+            if (j < m) {
+                const uint64_t x = a + j;
+                const uint32_t b = x >= vlo ? ring[idx(x)] : dst[x];
+                w[j >> 2] |= b << ((j & 3) * 8);
+            }
+        }
+        return make_uint4(w[0], w[1], w[2], w[3]);
+    }
+
+    // Write the first m (1..16) bytes of v at output position x (ring).
+    __device__ __forceinline__ void put16(uint64_t x, const uint4& v, uint32_t m) const {
+        const uint32_t ix = idx(x);
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (uint32_t j = 0; j < 16; ++j) {
+            if (j < m) ring[(ix + j) & (kRing - 1)] = static_cast<uint8_t>(w[j >> 2] >> ((j & 3) * 8));
+        }
+    }
+
+    // Copy positions [flushed, end) that are ready to the destination: the
+    // head up to the first aligned boundary and, when `final`, the tail by
+    // byte stores; whole aligned 16-byte blocks by coalesced vector stores.
+    __device__ __forceinline__ void flush(uint64_t end, bool final, uint32_t lane) {
+        const uint64_t f = flushed;
+        if (end <= f) return;
+        uint64_t fa = ((dbase + f + 15) & ~static_cast<uintptr_t>(15)) - dbase;
+        const uint64_t ea = ((dbase + end) & ~static_cast<uintptr_t>(15)) - dbase;
+        const uint64_t hend = fa < end ? fa : end;
+        if (f + lane < hend) dst[f + lane] = ring[idx(f + lane)];
+        uint64_t nf = hend;
+        if (ea > fa) {
+            for (uint64_t b = fa + 16ull * lane; b < ea; b += 16ull * 32)
+                *reinterpret_cast<uint4*>(dst + b) = *reinterpret_cast<const uint4*>(ring + idx(b));
+            nf = ea;
+        }
+        if (final && nf < end) {
+            if (nf + lane < end) dst[nf + lane] = ring[idx(nf + lane)];
+            nf = end;
+        }
+        flushed = nf;
+        __syncwarp();
+    }
+};
+
+// m (1..16) input bytes at position a, from the window when all of them
+// are there.
+__device__ __forceinline__ uint4 in16(const In& in, uint64_t a, uint32_t m) {
+    if (in.held(a, m)) {
+        const uint32_t ia = static_cast<uint32_t>((in.gbase + a) & (kIn - 1));
+        const uint32_t b0 = ia & ~15u, b1 = (b0 + 16) & (kIn - 1);
+        const uint4 lo = *reinterpret_cast<const uint4*>(in.win + b0);
+        const uint4 hi = *reinterpret_cast<const uint4*>(in.win + b1);
+        return shift32(lo, hi, ia & 15);
+    }
+    return ld16_input(in.g + a, m);
+}
+
+// Copy n input bytes from position src to output position o.
+__device__ __forceinline__ void copy_literal(const Out& out, const In& in, uint64_t src,
+                                             uint64_t o, uint64_t n) {
+    for (uint64_t k = 0; k < n; k += 16) {
+        const uint32_t m = n - k < 16 ? static_cast<uint32_t>(n - k) : 16u;
+        out.put16(o + k, in16(in, src + k, m), m);
+    }
+}
+
+// Output [o, o + n) = the match with offset off (out[x] = out[x - off]);
+// every source byte below o is already written.
+__device__ __forceinline__ void copy_match(const Out& out, uint64_t o, uint64_t n, uint32_t off) {
+    if (off >= 16) {
+        for (uint64_t k = 0; k < n; k += 16) {
+            const uint32_t m = n - k < 16 ? static_cast<uint32_t>(n - k) : 16u;
+            out.put16(o + k, out.fetch16(o + k - off, m), m);
+        }
+        return;
+    }
+    // Period off < 16: expand the period to a multiple P <= 16 in registers.
+    const uint4 v = out.fetch16(o - off, off);
+    uint32_t u[4] = {0, 0, 0, 0};
+    uint32_t k = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < 16; ++j) {
+        u[j >> 2] |= byte_of(v, k) << ((j & 3) * 8);
+        k = k + 1 == off ? 0 : k + 1;
+    }
+    const uint4 uv = make_uint4(u[0], u[1], u[2], u[3]);
+    const uint32_t P = off * (16 / off);
+    for (uint64_t x = 0; x < n; x += P) {
+        const uint32_t m = n - x < P ? static_cast<uint32_t>(n - x) : P;
+        out.put16(o + x, uv, m);
+    }
+}
+
+__device__ __forceinline__ uint64_t warp_min_u64(uint64_t v) {
+#pragma unroll
+    for (int s = 16; s; s >>= 1) {
+        const uint64_t o = __shfl_xor_sync(kFull, v, s);
+        v = o < v ? o : v;
+    }
+    return v;
+}
+
+// Input window filler: aligned 16-byte blocks of the chunk, by cp.async.
+// Only blocks holding at least one byte of [0, S) are read, so no load leaves
+// the 16-byte blocks the chunk itself occupies.
+struct Filler {
+    const uint8_t* g;
+    uint8_t* win;
+    uintptr_t gbase;
+    uint64_t S;
+    int64_t next;   // chunk-relative start of the next block to fetch
+    int64_t first;  // blocks [first, next) are fetched or in flight
+
+    // Issue fetches for the blocks from position `from` up to `until`
+    // (exclusive); blocks before `from` that were never fetched are skipped.
+    __device__ __forceinline__ void issue(uint64_t from, uint64_t until, uint32_t lane) {
+        if (S == 0) return;
+        const int64_t lim = static_cast<int64_t>(until < S ? until : S);
+        if (next < static_cast<int64_t>(from)) {
+            next = static_cast<int64_t>(from) - static_cast<int64_t>((gbase + from) & 15);
+            first = next;
+        }
+        if (next >= lim) return;
+        for (int64_t b = next + 16 * static_cast<int64_t>(lane); b < lim; b += 16 * 32) {
+            const uint8_t* src = g + b;  // 16-byte aligned by construction
+            uint8_t* dst = win + ((gbase + b) & (kIn - 1));
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)),
+                         "l"(src)
+                         : "memory");
+        }
+        next += ((lim - next + 15) / 16) * 16;
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+    // Lowest position that is fetched and whose slot no fetch issued so far
+    // overwrites.
+    __device__ __forceinline__ uint64_t low() const {
+        int64_t r = next - static_cast<int64_t>(kIn);
+        if (r < first) r = first;
+        return r > 0 ? static_cast<uint64_t>(r) : 0;
+    }
+    // Wait for everything issued; afterwards positions below the returned
+    // bound (and at or above low()) are in the window.
+    __device__ __forceinline__ uint64_t land() const {
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncwarp();
+        const int64_t r = next < static_cast<int64_t>(S) ? next : static_cast<int64_t>(S);
+        return r > 0 ? static_cast<uint64_t>(r) : 0;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Parallel token-chain parse over a window of kPW input positions starting at
+// a known token p: tab[0][i] = where the next token starts if one starts at
+// p + i (relative to p; kExit if it leaves the window or the input, or
+// cannot be a token),
+// tab[k] = 2^k steps. Lane l then finds the l-th token after a known one in
+// five lookups.
+__device__ __forceinline__ uint32_t hop(const uint16_t* tab, uint32_t t, uint32_t lane) {
+#pragma unroll
+    for (uint32_t b = 0; b < kLevels; ++b)
+        if (((lane >> b) & 1) && t != kExit) t = tab[b * kPW + t];
+    return t;
+}
+
+template <class F>
+__device__ __forceinline__ void build_tables(const In& in, uint64_t S, uint64_t p,
+                                             uint16_t* tab, uint32_t lane) {
+    LZW_T(t_step);
+#pragma unroll 4
+    for (uint32_t i = lane; i < kPW; i += 32) {
+        const uint64_t x = p + i;
+        uint32_t v = kExit;
+        if (x < S) {
+            const uint64_t nx = F::step(in, S, x);
+            if (nx != kNone && nx < S && nx - p < kPW) v = static_cast<uint32_t>(nx - p);
+        }
+        tab[i] = static_cast<uint16_t>(v);
+    }
+    __syncwarp();
+    LZW_ADD(4, t_step);
+    for (uint32_t b = 1; b < kLevels; ++b) {
+        const uint16_t* lo = tab + (b - 1) * kPW;
+        uint16_t* hi = tab + b * kPW;
+#pragma unroll 4
+        for (uint32_t i = lane; i < kPW; i += 32) {
+            const uint32_t a = lo[i];
+            hi[i] = a == kExit ? kExit : lo[a];
+        }
+        __syncwarp();
+    }
+}
+
+__device__ __forceinline__ uint64_t warp_incl_scan(uint64_t v, uint32_t lane) {
+#pragma unroll
+    for (uint32_t k = 1; k < 32; k <<= 1) {
+        const uint64_t o = __shfl_up_sync(kFull, v, k);
+        if (lane >= k) v += o;
+    }
+    return v;
+}
+
+// Store m (1..16) bytes of v at global p (16-byte store when aligned and whole).
+__device__ __forceinline__ void st16_global(uint8_t* p, const uint4& v, uint32_t m) {
+    if (m == 16 && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+        *reinterpret_cast<uint4*>(p) = v;
+        return;
+    }
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (uint32_t j = 0; j < 16; ++j)
+        if (j < m) p[j] = static_cast<uint8_t>(w[j >> 2] >> ((j & 3) * 8));
+}
+
+// The whole warp copies n input bytes at g + src to dst + o (no overlap):
+// destination-aligned 16-byte stores, four in flight per lane.
+__device__ __forceinline__ void coop_literal(uint8_t* dst, uint64_t o, const uint8_t* src, uint64_t n,
+                             uint32_t lane) {
+    uint8_t* D = dst + o;
+    uint64_t head = (16 - (reinterpret_cast<uintptr_t>(D) & 15)) & 15;
+    if (head > n) head = n;
+    if (lane < head) D[lane] = __ldg(src + lane);
+    const uint64_t body_end = head + ((n - head) & ~15ull);
+    uint64_t k = head + 16ull * lane;
+    for (; k + 3 * 512 < body_end; k += 4 * 512) {
+        const uint4 v0 = ld16_input(src + k, 16), v1 = ld16_input(src + k + 512, 16);
+        const uint4 v2 = ld16_input(src + k + 1024, 16), v3 = ld16_input(src + k + 1536, 16);
+        *reinterpret_cast<uint4*>(D + k) = v0;
+        *reinterpret_cast<uint4*>(D + k + 512) = v1;
+        *reinterpret_cast<uint4*>(D + k + 1024) = v2;
+        *reinterpret_cast<uint4*>(D + k + 1536) = v3;
+    }
+    for (; k < body_end; k += 512) *reinterpret_cast<uint4*>(D + k) = ld16_input(src + k, 16);
+    if (body_end + lane < n) D[body_end + lane] = __ldg(src + body_end + lane);
+}
+
+// The whole warp writes the match dst[ms, ms + n) with offset off; every byte
+// before ms is in dst. `scratch` (>= 512 bytes of shared memory, free) holds
+// a short period.
+__device__ __forceinline__ void coop_match(uint8_t* dst, uint64_t ms, uint64_t n, uint32_t off,
+                           uint8_t* scratch, uint32_t lane) {
+    uint8_t* D = dst + ms;
+    uint64_t head = (16 - (reinterpret_cast<uintptr_t>(D) & 15)) & 15;
+    if (head > n) head = n;
+    const uint64_t body_end = head + ((n - head) & ~15ull);
+    if (off >= 512) {
+        // A wave of 32 x 16 bytes never reads its own output.
+        if (lane < head) D[lane] = D[static_cast<int64_t>(lane) - off];
+        __syncwarp();
+        for (uint64_t w = head; w < body_end; w += 512) {
+            const uint64_t k = w + 16ull * lane;
+            if (k < body_end) {
+                const uint4 v = ld16_output(D + k - off, 16);
+                *reinterpret_cast<uint4*>(D + k) = v;
+            }
+            __syncwarp();
+        }
+        for (uint64_t k = body_end; k < n; ++k) {  // < 16 bytes, serial order
+            if (lane == 0) D[k] = D[k - off];
+            __syncwarp();
+        }
+        return;
+    }
+    // Period off < 512: stage it, then every byte is period[(x - ms) mod off].
+    for (uint32_t j = lane; j < off; j += 32) scratch[j] = D[static_cast<int64_t>(j) - off];
+    __syncwarp();
+    if (lane < head) D[lane] = scratch[lane % off];
+    for (uint64_t k = head + 16ull * lane; k < body_end; k += 512) {
+        uint32_t ph = static_cast<uint32_t>(k % off);
+        uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (uint32_t j = 0; j < 16; ++j) {
+            w[j >> 2] |= static_cast<uint32_t>(scratch[ph]) << ((j & 3) * 8);
+            ph = ph + 1 == off ? 0 : ph + 1;
+        }
+        *reinterpret_cast<uint4*>(D + k) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    if (body_end + lane < n) D[body_end + lane] = scratch[(body_end + lane) % off];
+    __syncwarp();
+}
+
+// Lane-parallel execution of tokens whose output fits one ring batch: each
+// active lane holds one token (literal li bytes from input lsrc to o, then a
+// match of mi bytes at offset off); bend = end of the batch's output.
+__device__ __forceinline__ void exec_small(Out& out, const In& in, bool act, uint64_t o,
+                                           uint64_t li, uint64_t lsrc, uint64_t mi,
+                                           uint32_t off, uint64_t bend, uint32_t lane) {
+    if (bend > out.vlo + kRing) out.vlo = bend - kRing;
+    const uint64_t ms = o + li;
+    if (act && li) copy_literal(out, in, lsrc, o, li);
+    __syncwarp();
+    bool pend = act && mi != 0;
+    // Each round finishes at least the pending match with the lowest start.
+    while (__any_sync(kFull, pend)) {
+        const uint64_t front = warp_min_u64(pend ? ms : ~0ull);
+        if (pend) {
+            const uint64_t src_end = ms - off + mi;
+            const uint64_t need = src_end < ms ? src_end : ms;
+            if (need <= front) {
+                copy_match(out, ms, mi, off);
+                pend = false;
+            }
+        }
+        __syncwarp();
+        LZW_EV(2, 1);
+    }
+    out.flush(bend, false, lane);
+}
+
+// Decode one chunk with the calling warp. Returns the status; *written is
+// the output length on success.
+template <class F>
+__device__ __forceinline__ int decode_chunk(const uint8_t* g, uint64_t S, uint8_t* dst, uint64_t cap,
+                            uint8_t* ring, uint8_t* win, uint16_t* tab, uint32_t lane,
+                            uint64_t* written) {
+    *written = 0;
+    uint64_t p, limit;
+    int status = F::begin(g, S, cap, &p, &limit);
+    if (status != CUDEC_OK) return status;
+
+    const uintptr_t gbase = reinterpret_cast<uintptr_t>(g);
+    Filler fill{g, win, gbase, S, -static_cast<int64_t>(gbase & 15),
+                -static_cast<int64_t>(gbase & 15)};
+    In in{g, win, gbase, 0, 0};
+    fill.issue(p, p + kInAhead, lane);
+    Out out{ring, dst, reinterpret_cast<uintptr_t>(dst), 0, 0};
+    uint64_t d = 0;  // output position of the next token; all before it executed
+    LZW_T(t_chunk);
+    for (;;) {
+        LZW_T(t_land);
+        uint64_t ready = fill.land();
+        // Refill ahead of the parse; it overwrites only positions before
+        // p - 64, and those leave the window's valid range.
+        fill.issue(p, p + kInAhead, lane);
+        in.lo = fill.low();
+        const uint64_t want = S - p < kPW + 64 ? S : p + kPW + 64;
+        if (ready < want) ready = fill.land();  // the parse jumped past the window
+        in.span = ready > in.lo ? ready - in.lo : 0;
+        LZW_ADD(0, t_land);
+        if (F::at_end(p, S)) {
+            status = F::finish(d, limit);
+            break;
+        }
+        LZW_T(t_tab);
+        build_tables<F>(in, S, p, tab, lane);
+        LZW_ADD(1, t_tab);
+        uint32_t base = 0;
+        bool last = false;
+        for (;;) {
+            LZW_T(t_grp);
+            // ---- the next (up to) 32 tokens of the chain, exactly checked
+            const uint32_t t = hop(tab, base, lane);
+            const bool valid = t != kExit;
+            const uint64_t x = p + t;
+            const uint64_t len = valid ? F::length(in, S, x) : 0;
+            const uint64_t dl = d + warp_incl_scan(len, lane) - len;
+            Seq sq{};
+            int st = CUDEC_OK;
+            if (valid) st = F::parse(in, S, limit, x, dl, &sq);
+            uint32_t m = __popc(__ballot_sync(kFull, valid));
+            const unsigned ev = __ballot_sync(kFull, valid && (st != CUDEC_OK || sq.done));
+            if (ev) {
+                const int e = __ffs(ev) - 1;
+                const int se = __shfl_sync(kFull, st, e);
+                if (se != CUDEC_OK) {
+                    asm volatile("cp.async.wait_all;" ::: "memory");
+                    return se;
+                }
+                m = e + 1;
+                last = true;
+            }
+            const bool act = lane < m;
+            const uint64_t tend = dl + sq.lit + sq.ml;
+            const uint64_t nxt = __shfl_sync(kFull, sq.next, m - 1);
+            const uint64_t dend = __shfl_sync(kFull, tend, m - 1);
+            LZW_ADD(2, t_grp);
+            LZW_EV(0, 1);
+            LZW_EV(1, m);
+            LZW_T(t_exec);
+            // ---- execute them in ring batches; long tokens by the warp ----
+            const bool big = act && sq.lit + sq.ml > kBig;
+            uint32_t s0 = 0;
+            while (s0 < m) {
+                const uint64_t os = __shfl_sync(kFull, dl, s0);
+                const unsigned cut =
+                    __ballot_sync(kFull, act && lane >= s0 && (big || tend - os > kBatchMax));
+                const uint32_t e = cut ? __ffs(cut) - 1 : m;
+                if (e == s0) {
+                    const uint64_t bo = os;
+                    const uint64_t bli = __shfl_sync(kFull, sq.lit, s0);
+                    const uint64_t bls = __shfl_sync(kFull, sq.lit_src, s0);
+                    const uint64_t bmi = __shfl_sync(kFull, sq.ml, s0);
+                    const uint32_t boff = __shfl_sync(kFull, sq.off, s0);
+                    out.flush(bo, true, lane);
+                    if (bli) coop_literal(dst, bo, g + bls, bli, lane);
+                    __syncwarp();
+                    if (bmi) coop_match(dst, bo + bli, bmi, boff, ring, lane);
+                    __syncwarp();
+                    out.flushed = out.vlo = bo + bli + bmi;
+                    LZW_EV(3, 1);
+                    ++s0;
+                    continue;
+                }
+                const uint64_t bend = __shfl_sync(kFull, tend, e - 1);
+                exec_small(out, in, act && lane >= s0 && lane < e, dl, sq.lit, sq.lit_src,
+                           sq.ml, sq.off, bend, lane);
+                s0 = e;
+            }
+            d = dend;
+            LZW_ADD(3, t_exec);
+            if (last) break;
+            if (m == 32 && nxt < S && nxt - p < kPW) {
+                base = static_cast<uint32_t>(nxt - p);
+                continue;
+            }
+            p = nxt;
+            break;
+        }
+        if (last) break;
+    }
+    if (status != CUDEC_OK) {
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        return status;
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    out.flush(d, true, lane);
+    LZW_ADD(5, t_chunk);
+    *written = d;
+    return CUDEC_OK;
+}
+
+template <class F>
+__global__ void __launch_bounds__(kThreads)
+    lz_warp_kernel(const void* const* src_ptrs, const size_t* src_sizes, void* const* dst_ptrs,
+                   const size_t* dst_caps, size_t n, cudec_chunk_result* results) {
+    extern __shared__ __align__(16) uint8_t lzw_smem[];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint8_t* base = lzw_smem + warp * kWarpSmem;
+    uint8_t* ring = base;
+    uint8_t* win = base + kRing;
+    uint16_t* tab = reinterpret_cast<uint16_t*>(base + kRing + kIn);
+    const size_t total = static_cast<size_t>(gridDim.x) * kWarps;
+    for (size_t c = static_cast<size_t>(blockIdx.x) * kWarps + warp; c < n; c += total) {
+        uint64_t written = 0;
+        const int st = decode_chunk<F>(static_cast<const uint8_t*>(src_ptrs[c]), src_sizes[c],
+                                       static_cast<uint8_t*>(dst_ptrs[c]), dst_caps[c], ring,
+                                       win, tab, lane, &written);
+        if (lane == 0) {
+            results[c].status = st;
+            results[c].reserved = 0;
+            results[c].bytes_written = st == CUDEC_OK ? written : 0;
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace lzw
+}  // namespace cdb
