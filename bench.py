@@ -23,6 +23,11 @@ the launch itself is bracketed by CUDA events on its stream.
             against the measured HBM copy bandwidth
   cpu_baseline  the reference's own host decoder (its twin, compiled from
             its sources) on all host cores, same chunks
+  mixed     the uneven mixed batch: 100,000 chunks, sizes lognormal (median
+            16 KiB, sigma 1.2, clamped to 256 B - 4 MiB), copy probability
+            uniform 0.2-0.8 per chunk, 5 % incompressible chunks, half LZ4 and
+            half Snappy; the persistent work-stealing plan (tuned once, CUDA
+            graph) against the plain path (one batch launch per format)
   per_format    the same measurement for raw Snappy (same content) and for
             Zstd: 4,096 frames of 1 MiB (1 MiB window, 128 KiB blocks, 10%
             repeated-byte runs, back-references up to 1 MiB), libzstd level 3
@@ -65,6 +70,8 @@ def parse_args():
     ap.add_argument("--chunks", type=int, default=N_CHUNKS,
                     help="chunk count (the headline workload is 1024; smaller "
                          "counts are for profiler captures)")
+    ap.add_argument("--mixed-chunks", type=int, default=100000,
+                    help="chunks of the uneven mixed LZ4+Snappy batch (0 skips it)")
     ap.add_argument("--zstd-frames", type=int, default=4096,
                     help="Zstd frames per batch (0 skips the Zstd legs)")
     ap.add_argument("--zstd-unique", type=int, default=128,
@@ -233,6 +240,83 @@ def run_reference(args, rank):
     }), flush=True)
 
 
+def time_region(torch, stream, flush, steps, warmup, body):
+    """Mean device time (ms) of body() on `stream`, L2 flushed before each."""
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            flush.zero_()
+            body()
+        for k in range(steps):
+            flush.zero_()
+            starts[k].record(stream)
+            body()
+            ends[k].record(stream)
+    stream.synchronize()
+    return sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / steps
+
+
+MIXED_SEED = 0xC0DEC2
+
+
+def run_mixed(torch, cd, DeviceBatch, args, dev, stream, flush, max_over_ranks, world, warm):
+    """Uneven LZ4+Snappy batch: persistent tuned plan vs per-format launches."""
+    from cudec_b200 import workload as W
+    n = args.mixed_chunks
+    raws, comps, fmts = W.mixed_batch(n, MIXED_SEED, formats=("lz4", "snappy"))
+    caps = [len(r) for r in raws]
+    out_bytes = int(sum(caps))
+    in_bytes = int(sum(len(c) for c in comps))
+    allb = DeviceBatch(comps, caps, device=dev, poison=None)
+    plan = cd.MixedPlan()
+    s = stream.cuda_stream
+    with torch.cuda.stream(stream):
+        assert allb.run_mixed(plan, fmts, stream, tune=True) == 0
+    tuning = plan.tuning()
+    res = allb.results()
+    assert (res["status"] == 0).all() and (res["bytes_written"] == np.array(caps)).all()
+    for i in range(0, n, max(n // 64, 1)):
+        o = int(allb.dst_offs[i])
+        assert allb.d_dst[o:o + caps[i]].cpu().numpy().tobytes() == raws[i].tobytes()
+    steps = max(args.steps // 50, 3)
+    p_ms = max_over_ranks(time_region(torch, stream, flush, steps, warm,
+                                      lambda: allb.run_mixed(plan, fmts, stream)))
+    res = allb.results()
+    assert (res["status"] == 0).all()
+    plan.close()
+    del allb
+    torch.cuda.empty_cache()
+    subs = []
+    for f in ("lz4", "snappy"):
+        idx = [i for i, x in enumerate(fmts) if x == f]
+        subs.append((f, DeviceBatch([comps[i] for i in idx], [caps[i] for i in idx],
+                                    device=dev, poison=None)))
+
+    def plain():
+        for f, b in subs:
+            assert b.run(f, stream) == 0
+
+    q_ms = max_over_ranks(time_region(torch, stream, flush, steps, warm, plain))
+    for f, b in subs:
+        assert (b.results()["status"] == 0).all()
+    del subs
+    torch.cuda.empty_cache()
+    sizes = np.array(caps)
+    return {
+        "value": round(world * out_bytes / (p_ms * 1e-3) / 1e9, 3), "unit": "GB/s",
+        "ms_per_step": round(p_ms, 3),
+        "plain_per_format_value": round(world * out_bytes / (q_ms * 1e-3) / 1e9, 3),
+        "plain_per_format_ms": round(q_ms, 3),
+        "chunks": n, "decompressed_bytes": out_bytes, "compressed_bytes": in_bytes,
+        "largest_chunk": int(sizes.max()), "median_chunk": int(np.median(sizes)),
+        "roofline_frac": round((in_bytes + out_bytes) / (p_ms * 1e-3) / 1e9 / peaks()[0], 5),
+        "tuning_per_bucket": [list(t) for t in tuning],
+        "path": "cudec_mixed_decompress (graph: order + persistent work-stealing kernel) vs "
+                "cudec_lz4_decompress_batch + cudec_snappy_decompress_batch",
+    }
+
+
 def time_device(torch, batch, fmt, stream, flush, steps, warmup):
     """Mean launch time (ms) of the batch entry, L2 flushed before each."""
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
@@ -319,6 +403,12 @@ def main():
     assert (sres["status"] == 0).all()
     s_in = sum(len(c) for c in scomps)
     del sbatch
+
+    # ---- uneven mixed batch: persistent plan vs one launch per format ----
+    mixed_line = None
+    if args.mixed_chunks > 0:
+        mixed_line = run_mixed(torch, cd, DeviceBatch, args, dev, stream, flush,
+                               max_over_ranks, world, warm)
 
     # ---- Zstd, 1 MiB frames at levels 3 and 19 ------------------------
     zstd_lines = {}
@@ -411,6 +501,7 @@ def main():
                            "roofline_frac": round((s_in + out_bytes) / (s_ms * 1e-3) / 1e9 / peak, 5)},
                 **zstd_lines,
             },
+            **({"mixed": mixed_line} if mixed_line else {}),
             "gpu_launches": args.steps,
             "clocks": clocks.summary(),
         }

@@ -55,6 +55,11 @@ SIGNATURES = {
     "cudec_zstd_workspace_bytes": (ctypes.c_size_t, [_SZ]),
     "cudec_zstd_decompress_batch": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P, _SZ, _P]),
     "cudec_zstd_decompress_batch_noalloc": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P]),
+    "cudec_mixed_plan_create": (ctypes.c_int, [_P]),
+    "cudec_mixed_plan_destroy": (ctypes.c_int, [_P]),
+    "cudec_mixed_decompress": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _SZ, _P, _P]),
+    "cudec_mixed_plan_tune": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _SZ, _P, _P]),
+    "cudec_mixed_plan_get_tuning": (ctypes.c_int, [_P, _P]),
     "cudec_lz4f_decompress": (ctypes.c_int, [_P, _SZ, _P, _SZ, _P]),
     "cudec_stream_ctx_create": (ctypes.c_int, [_P]),
     "cudec_lz4_decompress_stream_ctx": (ctypes.c_int, [_P, _P, _P, _P, _P, _SZ, ctypes.c_int, _P]),
@@ -161,6 +166,54 @@ class StreamContext:
     def close(self):
         if self.handle:
             lib().cudec_stream_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+FORMAT_LZ4, FORMAT_SNAPPY, FORMAT_ZSTD, FORMAT_GDEFLATE = 0, 1, 2, 3
+FORMAT_CODES = {"lz4": FORMAT_LZ4, "snappy": FORMAT_SNAPPY, "zstd": FORMAT_ZSTD,
+                "gdeflate": FORMAT_GDEFLATE}
+MIXED_BUCKETS = 6
+
+
+class MixedPlan:
+    """cudec_mixed_plan: persistent mixed-format decode with its autotuner.
+
+    Arguments of decode/tune are device addresses (ints) of the chunk tables
+    plus one format-code byte per chunk; stream is a raw cudaStream_t value.
+    """
+
+    def __init__(self):
+        h = ctypes.c_void_p()
+        st = lib().cudec_mixed_plan_create(ctypes.byref(h))
+        if st != OK:
+            raise RuntimeError("cudec_mixed_plan_create: %s" % STATUS_NAMES.get(st, st))
+        self.handle = h
+
+    def decode(self, src_ptrs, src_sizes, dst_ptrs, dst_caps, formats, n, results, stream=None):
+        return lib().cudec_mixed_decompress(self.handle, src_ptrs, src_sizes, dst_ptrs,
+                                            dst_caps, formats, n, results, stream)
+
+    def tune(self, src_ptrs, src_sizes, dst_ptrs, dst_caps, formats, n, results, stream=None):
+        return lib().cudec_mixed_plan_tune(self.handle, src_ptrs, src_sizes, dst_ptrs,
+                                           dst_caps, formats, n, results, stream)
+
+    def tuning(self):
+        """[(parse_window, lookahead, ring_batch)] per size bucket."""
+        out = (ctypes.c_uint32 * (3 * MIXED_BUCKETS))()
+        st = lib().cudec_mixed_plan_get_tuning(self.handle, out)
+        if st != OK:
+            raise RuntimeError("cudec_mixed_plan_get_tuning: %s" % STATUS_NAMES.get(st, st))
+        return [tuple(out[3 * b:3 * b + 3]) for b in range(MIXED_BUCKETS)]
+
+    def close(self):
+        if self.handle:
+            lib().cudec_mixed_plan_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -90,7 +90,7 @@ static cudec_status launch_lz(std::atomic<int>* ready, const void* const* src,
     const size_t want = (n + lzw::kWarps - 1) / lzw::kWarps;
     const unsigned grid = static_cast<unsigned>(want < max_blocks ? want : max_blocks);
     lzw::lz_warp_kernel<Fmt><<<grid, lzw::kThreads, lzw::kWarps * lzw::kWarpSmem, stream>>>(
-        src, src_sizes, dst, caps, n, results);
+        src, src_sizes, dst, caps, n, results, lzw::kDefaultTune);
     return cudaGetLastError() == cudaSuccess ? CUDEC_OK : CUDEC_ERR_CUDA;
 }
 

@@ -41,16 +41,30 @@ constexpr uint32_t kWarps = 4;               // warps per CTA
 constexpr uint32_t kThreads = 32 * kWarps;
 constexpr uint32_t kRing = 8192;             // output ring per warp (bytes)
 constexpr uint32_t kIn = 4096;               // input window per warp (bytes)
-constexpr uint32_t kInAhead = kIn - 64;      // fill up to this far past the parse
-constexpr uint32_t kBatchMax = 4096;         // output bytes staged per batch
+constexpr uint32_t kInAhead = kIn - 64;      // largest fill distance past the parse
+constexpr uint32_t kBatchMax = 4096;         // largest output staged per ring batch
 constexpr uint64_t kBig = 256;               // longer tokens are copied by the whole warp
-constexpr uint32_t kPW = 1024;               // parse window (token positions per table)
+constexpr uint32_t kPW = 1024;               // largest parse window (positions per table)
 constexpr uint32_t kLevels = 5;              // hop tables: 1, 2, 4, 8, 16 tokens
 constexpr uint32_t kExit = 0xFFFF;           // hop leaves the window
 constexpr uint32_t kWarpSmem = kRing + kIn + kLevels * kPW * 2;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint64_t kNone = ~0ull;            // no next token (speculative step)
 static_assert(kBatchMax + 16 <= kRing, "a batch never overwrites unflushed bytes");
+
+// Per-launch (or per size bucket) shape of the decode: parse window
+// (positions per hop table, <= kPW, a multiple of 32), input fill distance
+// past the parse (pw + 64 .. kInAhead) and output bytes per ring batch
+// (<= kBatchMax). Any values in range decode identically; they only move time.
+struct Tune {
+    uint32_t pw, ahead, batch;
+};
+constexpr Tune kDefaultTune{kPW, kInAhead, kBatchMax};
+
+__host__ __device__ constexpr bool tune_valid(const Tune& t) {
+    return t.pw >= 32 && t.pw <= kPW && t.pw % 32 == 0 && t.ahead >= t.pw + 64 &&
+           t.ahead <= kInAhead && t.batch >= 256 && t.batch <= kBatchMax;
+}
 
 // Profiling builds (-DCDB_PHASE_TIMING) accumulate per-phase SM cycles and
 // event counts over all chunks of a launch.
@@ -598,16 +612,16 @@ __device__ __forceinline__ uint32_t hop(const uint16_t* tab, uint32_t t, uint32_
 }
 
 template <class F>
-__device__ __forceinline__ void build_tables(const In& in, uint64_t S, uint64_t p,
+__device__ __forceinline__ void build_tables(const In& in, uint64_t S, uint64_t p, uint32_t pw,
                                              uint16_t* tab, uint32_t lane) {
     LZW_T(t_step);
 #pragma unroll 4
-    for (uint32_t i = lane; i < kPW; i += 32) {
+    for (uint32_t i = lane; i < pw; i += 32) {
         const uint64_t x = p + i;
         uint32_t v = kExit;
         if (x < S) {
             const uint64_t nx = F::step(in, S, x);
-            if (nx != kNone && nx < S && nx - p < kPW) v = static_cast<uint32_t>(nx - p);
+            if (nx != kNone && nx < S && nx - p < pw) v = static_cast<uint32_t>(nx - p);
         }
         tab[i] = static_cast<uint16_t>(v);
     }
@@ -617,7 +631,7 @@ __device__ __forceinline__ void build_tables(const In& in, uint64_t S, uint64_t 
         const uint16_t* lo = tab + (b - 1) * kPW;
         uint16_t* hi = tab + b * kPW;
 #pragma unroll 4
-        for (uint32_t i = lane; i < kPW; i += 32) {
+        for (uint32_t i = lane; i < pw; i += 32) {
             const uint32_t a = lo[i];
             hi[i] = a == kExit ? kExit : lo[a];
         }
@@ -745,8 +759,8 @@ __device__ __forceinline__ void exec_small(Out& out, const In& in, bool act, uin
 // the output length on success.
 template <class F>
 __device__ __forceinline__ int decode_chunk(const uint8_t* g, uint64_t S, uint8_t* dst, uint64_t cap,
-                            uint8_t* ring, uint8_t* win, uint16_t* tab, uint32_t lane,
-                            uint64_t* written) {
+                            uint8_t* ring, uint8_t* win, uint16_t* tab, const Tune& tn,
+                            uint32_t lane, uint64_t* written) {
     *written = 0;
     uint64_t p, limit;
     int status = F::begin(g, S, cap, &p, &limit);
@@ -756,7 +770,7 @@ __device__ __forceinline__ int decode_chunk(const uint8_t* g, uint64_t S, uint8_
     Filler fill{g, win, gbase, S, -static_cast<int64_t>(gbase & 15),
                 -static_cast<int64_t>(gbase & 15)};
     In in{g, win, gbase, 0, 0};
-    fill.issue(p, p + kInAhead, lane);
+    fill.issue(p, p + tn.ahead, lane);
     Out out{ring, dst, reinterpret_cast<uintptr_t>(dst), 0, 0};
     uint64_t d = 0;  // output position of the next token; all before it executed
     LZW_T(t_chunk);
@@ -765,9 +779,9 @@ __device__ __forceinline__ int decode_chunk(const uint8_t* g, uint64_t S, uint8_
         uint64_t ready = fill.land();
         // Refill ahead of the parse; it overwrites only positions before
         // p - 64, and those leave the window's valid range.
-        fill.issue(p, p + kInAhead, lane);
+        fill.issue(p, p + tn.ahead, lane);
         in.lo = fill.low();
-        const uint64_t want = S - p < kPW + 64 ? S : p + kPW + 64;
+        const uint64_t want = S - p < tn.pw + 64 ? S : p + tn.pw + 64;
         if (ready < want) ready = fill.land();  // the parse jumped past the window
         in.span = ready > in.lo ? ready - in.lo : 0;
         LZW_ADD(0, t_land);
@@ -776,7 +790,7 @@ __device__ __forceinline__ int decode_chunk(const uint8_t* g, uint64_t S, uint8_
             break;
         }
         LZW_T(t_tab);
-        build_tables<F>(in, S, p, tab, lane);
+        build_tables<F>(in, S, p, tn.pw, tab, lane);
         LZW_ADD(1, t_tab);
         uint32_t base = 0;
         bool last = false;
@@ -817,7 +831,7 @@ __device__ __forceinline__ int decode_chunk(const uint8_t* g, uint64_t S, uint8_
             while (s0 < m) {
                 const uint64_t os = __shfl_sync(kFull, dl, s0);
                 const unsigned cut =
-                    __ballot_sync(kFull, act && lane >= s0 && (big || tend - os > kBatchMax));
+                    __ballot_sync(kFull, act && lane >= s0 && (big || tend - os > tn.batch));
                 const uint32_t e = cut ? __ffs(cut) - 1 : m;
                 if (e == s0) {
                     const uint64_t bo = os;
@@ -843,7 +857,7 @@ __device__ __forceinline__ int decode_chunk(const uint8_t* g, uint64_t S, uint8_
             d = dend;
             LZW_ADD(3, t_exec);
             if (last) break;
-            if (m == 32 && nxt < S && nxt - p < kPW) {
+            if (m == 32 && nxt < S && nxt - p < tn.pw) {
                 base = static_cast<uint32_t>(nxt - p);
                 continue;
             }
@@ -866,7 +880,7 @@ __device__ __forceinline__ int decode_chunk(const uint8_t* g, uint64_t S, uint8_
 template <class F>
 __global__ void __launch_bounds__(kThreads)
     lz_warp_kernel(const void* const* src_ptrs, const size_t* src_sizes, void* const* dst_ptrs,
-                   const size_t* dst_caps, size_t n, cudec_chunk_result* results) {
+                   const size_t* dst_caps, size_t n, cudec_chunk_result* results, Tune tn) {
     extern __shared__ __align__(16) uint8_t lzw_smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint8_t* base = lzw_smem + warp * kWarpSmem;
@@ -878,7 +892,7 @@ __global__ void __launch_bounds__(kThreads)
         uint64_t written = 0;
         const int st = decode_chunk<F>(static_cast<const uint8_t*>(src_ptrs[c]), src_sizes[c],
                                        static_cast<uint8_t*>(dst_ptrs[c]), dst_caps[c], ring,
-                                       win, tab, lane, &written);
+                                       win, tab, tn, lane, &written);
         if (lane == 0) {
             results[c].status = st;
             results[c].reserved = 0;

@@ -1,0 +1,429 @@
+// Persistent mixed-format batch decode.
+//
+// One launch decodes a batch whose chunks are LZ4 blocks, raw Snappy blocks
+// and Zstd frames in any mix and of any sizes (a per-chunk format code). A
+// plan owns everything the launch needs so the call allocates nothing:
+//
+//   * a largest-first order of the chunks (by output capacity), built on the
+//     device by a counting sort over log2 size classes, so the longest
+//     chunks start first and the tail of the launch is short chunks;
+//   * a work counter: every warp of the persistent grid takes the next chunk
+//     of that order with one atomic add (work stealing), whatever its format;
+//   * per-warp Zstd literal slots;
+//   * the decode shape per size bucket (parse window, input lookahead, ring
+//     batch) chosen by cudec_mixed_plan_tune, which times candidate shapes on
+//     the caller's own chunks, bucket by bucket;
+//   * a CUDA graph of the whole sequence (counter reset, order kernels,
+//     decode kernel), captured once per argument set and replayed.
+//
+// Per-chunk statuses and bytes are exactly those of the per-format entries
+// (the same device decoders run); an unknown format code is
+// CUDEC_ERR_UNSUPPORTED for that chunk.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "cudec.h"
+#include "host_util.h"
+#include "launch.h"
+#include "lz_warp_kernel.cuh"
+#include "zstd_frame.cuh"
+
+namespace cdb {
+namespace mixed {
+
+constexpr uint32_t kWarps = 4;
+constexpr uint32_t kThreads = 32 * kWarps;
+constexpr uint32_t kWarpSmem = lzw::kWarpSmem > sizeof(zstd::WarpSmem)
+                                   ? lzw::kWarpSmem
+                                   : static_cast<uint32_t>(sizeof(zstd::WarpSmem));
+constexpr uint32_t kSmem = kWarps * kWarpSmem;
+constexpr int kBuckets = CUDEC_MIXED_BUCKETS;
+constexpr int kClasses = 64;  // floor(log2(capacity)) classes for the order
+static_assert(kWarpSmem % 16 == 0, "per-warp regions stay 16-byte aligned");
+
+// Tuning buckets by output capacity: < 4 KiB, < 16 KiB, < 64 KiB, < 256 KiB,
+// < 1 MiB, larger.
+__host__ __device__ inline int size_bucket(uint64_t cap) {
+    return cap < 4096 ? 0 : cap < 16384 ? 1 : cap < 65536 ? 2 : cap < 262144 ? 3
+         : cap < 1048576 ? 4 : 5;
+}
+
+__device__ __forceinline__ int size_class(uint64_t cap) {
+    return cap ? 63 - __clzll(static_cast<long long>(cap)) : 0;
+}
+
+struct Args {
+    const void* const* src;
+    const size_t* sizes;
+    void* const* dst;
+    const size_t* caps;
+    const uint8_t* formats;
+    size_t n;
+    cudec_chunk_result* results;
+    const uint32_t* order;
+    unsigned long long* counter;
+    uint8_t* zstd_slots;
+    lzw::Tune tune[kBuckets];
+};
+
+// Control block in device memory: work counter, class counts, class cursors.
+struct Ctrl {
+    unsigned long long counter;
+    unsigned long long counts[kClasses];
+    unsigned long long cursor[kClasses];
+};
+
+__global__ void order_count(const size_t* caps, size_t n, Ctrl* ctrl) {
+    __shared__ unsigned int h[kClasses];
+    for (uint32_t i = threadIdx.x; i < kClasses; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x)
+        atomicAdd(&h[size_class(caps[i])], 1u);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < kClasses; i += blockDim.x)
+        if (h[i]) atomicAdd(&ctrl->counts[i], static_cast<unsigned long long>(h[i]));
+}
+
+// Start of each class in the order, largest class first (one thread).
+__global__ void order_scan(Ctrl* ctrl) {
+    if (threadIdx.x != 0) return;
+    unsigned long long at = 0;
+    for (int c = kClasses - 1; c >= 0; --c) {
+        ctrl->cursor[c] = at;
+        at += ctrl->counts[c];
+    }
+}
+
+__global__ void order_place(const size_t* caps, size_t n, Ctrl* ctrl, uint32_t* order) {
+    for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const unsigned long long at = atomicAdd(&ctrl->cursor[size_class(caps[i])], 1ull);
+        order[at] = static_cast<uint32_t>(i);
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) mixed_kernel(Args a) {
+    extern __shared__ __align__(16) uint8_t mixed_smem[];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint8_t* base = mixed_smem + warp * kWarpSmem;
+    const size_t gw = static_cast<size_t>(blockIdx.x) * kWarps + warp;
+    uint8_t* litbuf = a.zstd_slots + gw * zstd::kLitSlot;
+    for (;;) {
+        unsigned long long idx = 0;
+        if (lane == 0) idx = atomicAdd(a.counter, 1ull);
+        idx = __shfl_sync(0xffffffffu, idx, 0);
+        if (idx >= a.n) break;
+        const uint32_t c = a.order[idx];
+        const uint8_t* src = static_cast<const uint8_t*>(a.src[c]);
+        const uint64_t S = a.sizes[c], cap = a.caps[c];
+        uint8_t* dst = static_cast<uint8_t*>(a.dst[c]);
+        uint64_t written = 0;
+        int st;
+        switch (a.formats[c]) {
+            case CUDEC_FORMAT_LZ4:
+                st = lzw::decode_chunk<lzw::Lz4>(
+                    src, S, dst, cap, base, base + lzw::kRing,
+                    reinterpret_cast<uint16_t*>(base + lzw::kRing + lzw::kIn),
+                    a.tune[size_bucket(cap)], lane, &written);
+                break;
+            case CUDEC_FORMAT_SNAPPY:
+                st = lzw::decode_chunk<lzw::Snappy>(
+                    src, S, dst, cap, base, base + lzw::kRing,
+                    reinterpret_cast<uint16_t*>(base + lzw::kRing + lzw::kIn),
+                    a.tune[size_bucket(cap)], lane, &written);
+                break;
+            case CUDEC_FORMAT_ZSTD:
+                st = zstd::decode_frame(src, S, dst, cap, *reinterpret_cast<zstd::WarpSmem*>(base),
+                                        litbuf, lane, &written);
+                break;
+            default:
+                st = CUDEC_ERR_UNSUPPORTED;
+                break;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            a.results[c].status = st;
+            a.results[c].reserved = 0;
+            a.results[c].bytes_written = st == CUDEC_OK ? written : 0;
+        }
+    }
+}
+
+struct Key {
+    const void* const* src;
+    const size_t* sizes;
+    void* const* dst;
+    const size_t* caps;
+    const uint8_t* formats;
+    size_t n;
+    cudec_chunk_result* results;
+    bool operator==(const Key& o) const {
+        return src == o.src && sizes == o.sizes && dst == o.dst && caps == o.caps &&
+               formats == o.formats && n == o.n && results == o.results;
+    }
+};
+
+}  // namespace mixed
+}  // namespace cdb
+
+struct cudec_mixed_plan {
+    int dev = -1;
+    unsigned grid = 0;
+    int sms = 0;
+    cdb::DevBuf ctrl, order, slots;
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr, t0 = nullptr, t1 = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cdb::mixed::Key key{};
+    cdb::lzw::Tune tune[cdb::mixed::kBuckets];
+
+    void drop_graph() {
+        if (exec) (void)cudaGraphExecDestroy(exec);
+        if (graph) (void)cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+    }
+    ~cudec_mixed_plan() {
+        if (s) (void)cudaStreamSynchronize(s);
+        drop_graph();
+        for (cudaEvent_t e : {ev_in, ev_out, t0, t1})
+            if (e) (void)cudaEventDestroy(e);
+        if (s) (void)cudaStreamDestroy(s);
+    }
+};
+
+namespace {
+
+using cdb::mixed::Args;
+using cdb::mixed::Ctrl;
+using cdb::mixed::Key;
+
+cudec_status check_args(const cudec_mixed_plan* plan, const void* const* src,
+                        const size_t* sizes, void* const* dst, const size_t* caps,
+                        const uint8_t* formats, size_t n, const cudec_chunk_result* results) {
+    if (plan == nullptr || formats == nullptr || n > 0xFFFFFFFFull)
+        return CUDEC_ERR_INVALID_ARGUMENT;
+    return cdb::validate_batch(src, sizes, dst, caps, n, results);
+}
+
+Args make_args(cudec_mixed_plan* p, const Key& k) {
+    Args a{};
+    a.src = k.src;
+    a.sizes = k.sizes;
+    a.dst = k.dst;
+    a.caps = k.caps;
+    a.formats = k.formats;
+    a.n = k.n;
+    a.results = k.results;
+    a.order = static_cast<const uint32_t*>(p->order.p);
+    a.counter = &static_cast<Ctrl*>(p->ctrl.p)->counter;
+    a.zstd_slots = static_cast<uint8_t*>(p->slots.p);
+    for (int b = 0; b < cdb::mixed::kBuckets; ++b) a.tune[b] = p->tune[b];
+    return a;
+}
+
+// The whole decode of one batch on stream s: order, then the persistent grid.
+cudaError_t enqueue(cudec_mixed_plan* p, const Key& k, cudaStream_t s) {
+    Ctrl* ctrl = static_cast<Ctrl*>(p->ctrl.p);
+    cudaError_t e = cudaMemsetAsync(ctrl, 0, sizeof(Ctrl), s);
+    if (e != cudaSuccess) return e;
+    const size_t want = (k.n + 255) / 256;
+    const unsigned blocks = static_cast<unsigned>(std::min<size_t>(want, 4u * p->sms));
+    cdb::mixed::order_count<<<blocks, 256, 0, s>>>(k.caps, k.n, ctrl);
+    cdb::mixed::order_scan<<<1, 32, 0, s>>>(ctrl);
+    cdb::mixed::order_place<<<blocks, 256, 0, s>>>(k.caps, k.n, ctrl,
+                                                    static_cast<uint32_t*>(p->order.p));
+    cdb::mixed::mixed_kernel<<<p->grid, cdb::mixed::kThreads, cdb::mixed::kSmem, s>>>(
+        make_args(p, k));
+    return cudaGetLastError();
+}
+
+cudec_status bind(cudec_mixed_plan* p, size_t n) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return CUDEC_ERR_CUDA;
+    if (dev != p->dev) return CUDEC_ERR_INVALID_ARGUMENT;
+    if (p->order.cap < n * sizeof(uint32_t)) {
+        p->drop_graph();
+        if (p->order.ensure(n * sizeof(uint32_t)) != cudaSuccess) return CUDEC_ERR_CUDA;
+    }
+    return CUDEC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+cudec_status cudec_mixed_plan_create(cudec_mixed_plan** out_plan) {
+    if (out_plan == nullptr) return CUDEC_ERR_INVALID_ARGUMENT;
+    *out_plan = nullptr;
+    (void)cudaGetLastError();
+    cudec_mixed_plan* p = new (std::nothrow) cudec_mixed_plan();
+    if (p == nullptr) return CUDEC_ERR_CUDA;
+    for (int b = 0; b < cdb::mixed::kBuckets; ++b) p->tune[b] = cdb::lzw::kDefaultTune;
+    int per_sm = 0;
+    bool ok = cudaGetDevice(&p->dev) == cudaSuccess;
+    ok = ok && (p->sms = cdb::device_sm_count(p->dev)) > 0;
+    ok = ok && cudaFuncSetAttribute(cdb::mixed::mixed_kernel,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(cdb::mixed::kSmem)) == cudaSuccess;
+    ok = ok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cdb::mixed::mixed_kernel,
+                                                             cdb::mixed::kThreads,
+                                                             cdb::mixed::kSmem) == cudaSuccess;
+    ok = ok && per_sm > 0;
+    if (ok) p->grid = static_cast<unsigned>(p->sms * per_sm);
+    ok = ok && p->ctrl.ensure(sizeof(Ctrl)) == cudaSuccess;
+    ok = ok && p->slots.ensure(static_cast<size_t>(p->grid) * cdb::mixed::kWarps *
+                               cdb::zstd::kLitSlot) == cudaSuccess;
+    ok = ok && cudaStreamCreateWithFlags(&p->s, cudaStreamNonBlocking) == cudaSuccess;
+    for (cudaEvent_t* e : {&p->ev_in, &p->ev_out})
+        ok = ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
+    for (cudaEvent_t* e : {&p->t0, &p->t1}) ok = ok && cudaEventCreate(e) == cudaSuccess;
+    if (!ok) {
+        delete p;
+        (void)cudaGetLastError();
+        return CUDEC_ERR_CUDA;
+    }
+    *out_plan = p;
+    return CUDEC_OK;
+}
+
+cudec_status cudec_mixed_plan_destroy(cudec_mixed_plan* plan) {
+    if (plan == nullptr) return CUDEC_ERR_INVALID_ARGUMENT;
+    delete plan;
+    return CUDEC_OK;
+}
+
+cudec_status cudec_mixed_decompress(cudec_mixed_plan* plan, const void* const* d_src_ptrs,
+                                    const size_t* d_src_sizes, void* const* d_dst_ptrs,
+                                    const size_t* d_dst_capacities, const uint8_t* d_formats,
+                                    size_t chunk_count, cudec_chunk_result* d_results,
+                                    cudec_stream_t stream) {
+    const cudec_status v = check_args(plan, d_src_ptrs, d_src_sizes, d_dst_ptrs,
+                                      d_dst_capacities, d_formats, chunk_count, d_results);
+    if (v != CUDEC_OK) return v;
+    (void)cudaGetLastError();
+    const cudec_status b = bind(plan, chunk_count);
+    if (b != CUDEC_OK) return b;
+    const Key k{d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_capacities,
+                d_formats, chunk_count, d_results};
+    if (plan->exec == nullptr || !(plan->key == k)) {
+        plan->drop_graph();
+        if (cudaStreamBeginCapture(plan->s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return CUDEC_ERR_CUDA;
+        const cudaError_t ce = enqueue(plan, k, plan->s);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(plan->s, &g);
+        if (ce != cudaSuccess || ee != cudaSuccess || g == nullptr) {
+            if (g) (void)cudaGraphDestroy(g);
+            (void)cudaGetLastError();
+            return CUDEC_ERR_CUDA;
+        }
+        plan->graph = g;
+        if (cudaGraphInstantiate(&plan->exec, g, 0) != cudaSuccess) {
+            plan->drop_graph();
+            (void)cudaGetLastError();
+            return CUDEC_ERR_CUDA;
+        }
+        plan->key = k;
+    }
+    const cudaStream_t cs = reinterpret_cast<cudaStream_t>(stream);
+    bool ok = cudaEventRecord(plan->ev_in, cs) == cudaSuccess;
+    ok = ok && cudaStreamWaitEvent(plan->s, plan->ev_in, 0) == cudaSuccess;
+    ok = ok && cudaGraphLaunch(plan->exec, plan->s) == cudaSuccess;
+    ok = ok && cudaEventRecord(plan->ev_out, plan->s) == cudaSuccess;
+    ok = ok && cudaStreamWaitEvent(cs, plan->ev_out, 0) == cudaSuccess;
+    return ok ? CUDEC_OK : CUDEC_ERR_CUDA;
+}
+
+cudec_status cudec_mixed_plan_tune(cudec_mixed_plan* plan, const void* const* d_src_ptrs,
+                                   const size_t* d_src_sizes, void* const* d_dst_ptrs,
+                                   const size_t* d_dst_capacities, const uint8_t* d_formats,
+                                   size_t chunk_count, cudec_chunk_result* d_results,
+                                   cudec_stream_t stream) {
+    const cudec_status v = check_args(plan, d_src_ptrs, d_src_sizes, d_dst_ptrs,
+                                      d_dst_capacities, d_formats, chunk_count, d_results);
+    if (v != CUDEC_OK) return v;
+    (void)cudaGetLastError();
+    const cudec_status b = bind(plan, chunk_count);
+    if (b != CUDEC_OK) return b;
+    const cudaStream_t cs = reinterpret_cast<cudaStream_t>(stream);
+    if (cudaStreamSynchronize(cs) != cudaSuccess) return CUDEC_ERR_CUDA;
+    std::vector<size_t> caps(chunk_count);
+    if (cudaMemcpy(caps.data(), d_dst_capacities, chunk_count * sizeof(size_t),
+                   cudaMemcpyDeviceToHost) != cudaSuccess)
+        return CUDEC_ERR_CUDA;
+    std::vector<std::vector<uint32_t>> members(cdb::mixed::kBuckets);
+    for (size_t i = 0; i < chunk_count; ++i)
+        members[cdb::mixed::size_bucket(caps[i])].push_back(static_cast<uint32_t>(i));
+    std::vector<cdb::lzw::Tune> cands;
+    for (uint32_t pw : {256u, 512u, 1024u})
+        for (uint32_t ahead : {std::min(2 * pw + 64, cdb::lzw::kInAhead), cdb::lzw::kInAhead})
+            for (uint32_t batch : {2048u, 4096u}) {
+                const cdb::lzw::Tune t{pw, ahead, batch};
+                bool dup = false;
+                for (const auto& c : cands)
+                    dup = dup || (c.pw == t.pw && c.ahead == t.ahead && c.batch == t.batch);
+                if (!dup && cdb::lzw::tune_valid(t)) cands.push_back(t);
+            }
+    plan->drop_graph();
+    const Key whole{d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_capacities,
+                    d_formats, chunk_count, d_results};
+    Ctrl* ctrl = static_cast<Ctrl*>(plan->ctrl.p);
+    for (int bk = 0; bk < cdb::mixed::kBuckets; ++bk) {
+        const std::vector<uint32_t>& m = members[bk];
+        if (m.empty()) continue;
+        if (cudaMemcpyAsync(plan->order.p, m.data(), m.size() * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice, plan->s) != cudaSuccess)
+            return CUDEC_ERR_CUDA;
+        float best = 0.f;
+        cdb::lzw::Tune best_t = plan->tune[bk];
+        for (const auto& t : cands) {
+            Args a = make_args(plan, whole);
+            a.n = m.size();
+            for (int q = 0; q < cdb::mixed::kBuckets; ++q) a.tune[q] = t;
+            float ms_min = 0.f;
+            for (int rep = 0; rep < 2; ++rep) {
+                bool ok = cudaMemsetAsync(&ctrl->counter, 0, sizeof(ctrl->counter), plan->s) ==
+                          cudaSuccess;
+                ok = ok && cudaEventRecord(plan->t0, plan->s) == cudaSuccess;
+                cdb::mixed::mixed_kernel<<<plan->grid, cdb::mixed::kThreads, cdb::mixed::kSmem,
+                                           plan->s>>>(a);
+                ok = ok && cudaGetLastError() == cudaSuccess;
+                ok = ok && cudaEventRecord(plan->t1, plan->s) == cudaSuccess;
+                ok = ok && cudaEventSynchronize(plan->t1) == cudaSuccess;
+                float ms = 0.f;
+                ok = ok && cudaEventElapsedTime(&ms, plan->t0, plan->t1) == cudaSuccess;
+                if (!ok) {
+                    (void)cudaGetLastError();
+                    return CUDEC_ERR_CUDA;
+                }
+                if (rep == 0 || ms < ms_min) ms_min = ms;
+            }
+            if (best == 0.f || ms_min < best) {
+                best = ms_min;
+                best_t = t;
+            }
+        }
+        plan->tune[bk] = best_t;
+    }
+    return cudaStreamSynchronize(plan->s) == cudaSuccess ? CUDEC_OK : CUDEC_ERR_CUDA;
+}
+
+cudec_status cudec_mixed_plan_get_tuning(const cudec_mixed_plan* plan, uint32_t* out_params) {
+    if (plan == nullptr || out_params == nullptr) return CUDEC_ERR_INVALID_ARGUMENT;
+    for (int b = 0; b < cdb::mixed::kBuckets; ++b) {
+        out_params[3 * b] = plan->tune[b].pw;
+        out_params[3 * b + 1] = plan->tune[b].ahead;
+        out_params[3 * b + 2] = plan->tune[b].batch;
+    }
+    return CUDEC_OK;
+}
+
+}  // extern "C"

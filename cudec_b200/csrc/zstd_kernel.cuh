@@ -135,7 +135,7 @@ struct DescIn {
 };
 
 // FSE description (src/zstd_fse.h ZstdFseReadNCount). Returns false on reject.
-__device__ bool fse_ncount(const uint8_t* src, uint64_t size, unsigned max_sym,
+__device__ inline bool fse_ncount(const uint8_t* src, uint64_t size, unsigned max_sym,
                            unsigned max_log, int16_t* counts, unsigned* out_max,
                            unsigned* out_log, uint64_t* used) {
     if (size == 0) return false;
@@ -200,7 +200,7 @@ __device__ bool fse_ncount(const uint8_t* src, uint64_t size, unsigned max_sym,
 
 // Table spread and cells (src/zstd_fse.h ZstdFseBuildDTable); all lanes run
 // it redundantly, lane 0 writes.
-__device__ bool fse_build(const int16_t* counts, unsigned max_sym, unsigned log,
+__device__ inline bool fse_build(const int16_t* counts, unsigned max_sym, unsigned log,
                           uint32_t* cells, uint16_t* next, uint32_t lane) {
     const uint32_t size = 1u << log;
     uint32_t claimed = 0;
@@ -257,7 +257,7 @@ __device__ bool fse_build(const int16_t* counts, unsigned max_sym, unsigned log,
 }
 
 // Huffman weights (src/zstd_huf.h ZstdHufReadWeights, literals cap 11).
-__device__ bool huf_weights(const uint8_t* src, uint64_t size, WarpSmem& w, uint32_t lane,
+__device__ inline bool huf_weights(const uint8_t* src, uint64_t size, WarpSmem& w, uint32_t lane,
                             unsigned* count, unsigned* table_log, uint64_t* used) {
     if (size == 0) return false;
     const unsigned hdr = src[0];
@@ -340,7 +340,7 @@ __device__ bool huf_weights(const uint8_t* src, uint64_t size, WarpSmem& w, uint
 
 // Decoding table from weights (src/zstd_huf.h ZstdHufBuildDTable): symbols in
 // weight order, each weight-w symbol spans 2^(w-1) cells of tl+1-w bits.
-__device__ bool huf_build(WarpSmem& w, unsigned count, unsigned tl, uint32_t lane) {
+__device__ inline bool huf_build(WarpSmem& w, unsigned count, unsigned tl, uint32_t lane) {
     const uint8_t* wt = w.weights;
     const uint32_t size = 1u << tl;
     uint32_t rc[13];
@@ -389,7 +389,7 @@ __device__ bool huf_build(WarpSmem& w, unsigned count, unsigned tl, uint32_t lan
 }
 
 // One Huffman stream of `count` symbols; writes to dst when non-null.
-__device__ bool huf_stream(const uint8_t* src, uint64_t size, const uint16_t* huf, unsigned tl,
+__device__ inline bool huf_stream(const uint8_t* src, uint64_t size, const uint16_t* huf, unsigned tl,
                            uint8_t* dst, uint64_t count) {
     BitIn r;
     if (!r.start(src, size)) return false;
@@ -410,18 +410,18 @@ __device__ __forceinline__ unsigned ml_bits(unsigned c) {
          : (c < 36 ? 1 : c < 38 ? 2 : c < 40 ? 3 : c < 42 ? 4 : 5);
 }
 // Baselines: code c's base is the sum of 2^extra over the codes below it.
-__constant__ uint32_t kLLBase[36] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15,
+static __constant__ uint32_t kLLBase[36] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15,
                                      16, 18, 20, 22, 24, 28, 32, 40, 48, 64, 128, 256, 512,
                                      1024, 2048, 4096, 8192, 16384, 32768, 65536};
-__constant__ uint32_t kMLBase[53] = {3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18,
+static __constant__ uint32_t kMLBase[53] = {3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18,
                                      19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29, 30, 31, 32,
                                      33, 34, 35, 37, 39, 41, 43, 47, 51, 59, 67, 83, 99, 131,
                                      259, 515, 1027, 2051, 4099, 8195, 16387, 32771, 65539};
-__constant__ int16_t kPreLL[36] = {4, 3, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 1, 1, 1, 2, 2,
+static __constant__ int16_t kPreLL[36] = {4, 3, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 1, 1, 1, 2, 2,
                                    2, 2, 2, 2, 2, 2, 2, 3, 2, 1, 1, 1, 1, 1, -1, -1, -1, -1};
-__constant__ int16_t kPreOF[29] = {1, 1, 1, 1, 1, 1, 2, 2, 2, 1, 1, 1, 1, 1, 1,
+static __constant__ int16_t kPreOF[29] = {1, 1, 1, 1, 1, 1, 2, 2, 2, 1, 1, 1, 1, 1, 1,
                                    1, 1, 1, 1, 1, 1, 1, 1, 1, -1, -1, -1, -1, -1};
-__constant__ int16_t kPreML[53] = {1, 4, 3, 2, 2, 2, 2, 2, 2, 1, 1, 1, 1, 1, 1, 1, 1, 1,
+static __constant__ int16_t kPreML[53] = {1, 4, 3, 2, 2, 2, 2, 2, 2, 1, 1, 1, 1, 1, 1, 1, 1, 1,
                                    1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1,
                                    1, 1, 1, 1, 1, 1, 1, 1, 1, 1, -1, -1, -1, -1, -1, -1, -1};
 
@@ -434,7 +434,7 @@ struct Tables {
 };
 
 // Sequence table load (src/zstd_seq.h ZstdSeqLoadTable).
-__device__ bool seq_table(WarpSmem& w, Tables& t, unsigned field, unsigned mode,
+__device__ inline bool seq_table(WarpSmem& w, Tables& t, unsigned field, unsigned mode,
                           const uint8_t* src, uint64_t size, uint64_t* used, uint32_t lane) {
     const unsigned symmax = field == 0 ? 35 : field == 1 ? 31 : 52;
     const unsigned logmax = field == 1 ? 8 : 9;
@@ -478,8 +478,6 @@ __device__ __forceinline__ void copy_bytes(uint8_t* dst, const uint8_t* src, uin
     for (uint64_t i = 0; i < n; ++i) dst[i] = src[i];
 }
 
-// XXH64 of dst[0, n) (public xxHash specification), one lane.
-__device__ uint64_t xxh64_dev(const uint8_t* p, uint64_t n);
 
 }  // namespace zstd
 }  // namespace cdb

@@ -80,6 +80,17 @@ class DeviceBatch:
             return cd.zstd_decompress_batch(*self.args(), ws.data_ptr(), ws.numel(), s)
         return cd.BATCH_ENTRIES[fmt](*self.args(), s)
 
+    def run_mixed(self, plan, formats, stream=None, tune=False):
+        """Decode through a MixedPlan; `formats` = one format code per chunk."""
+        s = (stream or torch.cuda.current_stream(self.device)).cuda_stream
+        if getattr(self, "_fmt_codes", None) is None or len(self._fmt_codes_src) != self.n or \
+                list(self._fmt_codes_src) != list(formats):
+            self._fmt_codes_src = list(formats)
+            self._fmt_codes = torch.tensor([cd.FORMAT_CODES.get(f, f) if isinstance(f, str) else f
+                                            for f in formats], dtype=torch.uint8).to(self.device)
+        fn = plan.tune if tune else plan.decode
+        return fn(*self.args()[:4], self._fmt_codes.data_ptr(), self.n, _ptr(self.d_results), s)
+
     def workspace(self):
         """Device workspace for the Zstd entry (allocated once per batch)."""
         if getattr(self, "_ws", None) is None:

@@ -248,3 +248,40 @@ def zstd_params(copy_prob=0.5, rle_prob=0.1):
     """Zstd content: the LZ content generator with back-references up to
     1 MiB and 10 % of events a run of one repeated byte (mean 64)."""
     return GenParams(copy_prob, 64, 1.1, 8.0, 16.0, 4, 255, 1 << 20, rle_prob, 64.0, 0)
+
+
+def mixed_sizes(n, seed, median=16384, sigma=1.2, lo=256, hi=4 << 20):
+    """Lognormal chunk sizes (median, sigma), clamped to [lo, hi]."""
+    rng = np.random.default_rng(seed)
+    s = np.exp(np.log(median) + sigma * rng.standard_normal(n))
+    return np.clip(s, lo, hi).astype(np.int64)
+
+
+def mixed_batch(n, seed, formats=("lz4", "snappy"), median=16384, sigma=1.2, lo=256,
+                hi=4 << 20, random_frac=0.05, threads=None):
+    """The uneven mixed batch: lognormal sizes, copy probability uniform in
+    0.2-0.8 per chunk, `random_frac` of the chunks uniform random bytes, the
+    format of chunk i = formats[i % len(formats)]. Returns (raws, comps, fmts)
+    with raws as numpy views of one buffer."""
+    sizes = mixed_sizes(n, seed, median, sigma, lo, hi)
+    rng = np.random.default_rng(seed + 1)
+    probs = rng.uniform(0.2, 0.8, n)
+    rand = rng.random(n) < random_frac
+    fmts = [formats[i % len(formats)] for i in range(n)]
+    params = [(zstd_params(float(p), 0.1) if f == "zstd" else lz_params(float(p), bool(r)))
+              for p, r, f in zip(probs, rand, fmts)]
+    for i, f in enumerate(fmts):
+        if f == "zstd" and rand[i]:
+            params[i] = lz_params(float(probs[i]), True)
+    seeds = np.array([chunk_seed(seed, 2, i) for i in range(n)], dtype=np.uint64)
+    buf, offs = generate(sizes, params, param_idx=np.arange(n), seeds=seeds, threads=threads)
+    raws = [buf[int(o):int(o) + int(s)] for o, s in zip(offs, sizes)]
+    comps = []
+    for r, f in zip(raws, fmts):
+        if f == "lz4":
+            comps.append(lz4_compress(r))
+        elif f == "snappy":
+            comps.append(snappy_compress(r))
+        else:
+            comps.append(zstd_compress(r.tobytes(), 3, 20, True))
+    return raws, comps, fmts

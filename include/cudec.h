@@ -158,6 +158,61 @@ cudec_status cudec_zstd_decompress_batch_noalloc(const void* const* d_src_ptrs,
                                                  cudec_stream_t stream);
 
 /* ---------------------------------------------------------------------
+ * Mixed-format persistent batch decode (no counterpart in the reference; the
+ * design record's batching direction). One launch decodes LZ4 blocks, raw
+ * Snappy blocks and Zstd frames in any mix, with per-chunk statuses and bytes
+ * identical to the per-format entries. A plan (bound to the device current at
+ * creation) owns the device workspace (work counter, a largest-first chunk
+ * order, Zstd literal slots), the decode shape per size bucket and a CUDA
+ * graph of the launch sequence, captured once per argument set and replayed.
+ * d_formats holds one cudec_format code per chunk; an unknown code is
+ * CUDEC_ERR_UNSUPPORTED for that chunk. chunk_count <= 2^32 - 1. Calls on one
+ * plan are serialised on its private stream and ordered after `stream`. */
+typedef enum cudec_format {
+    CUDEC_FORMAT_LZ4 = 0,
+    CUDEC_FORMAT_SNAPPY = 1,
+    CUDEC_FORMAT_ZSTD = 2,
+    CUDEC_FORMAT_GDEFLATE = 3
+} cudec_format;
+
+/* Size buckets of the tuned decode shape, by output capacity: < 4 KiB,
+ * < 16 KiB, < 64 KiB, < 256 KiB, < 1 MiB, larger. */
+#define CUDEC_MIXED_BUCKETS 6
+
+typedef struct cudec_mixed_plan cudec_mixed_plan;
+
+cudec_status cudec_mixed_plan_create(cudec_mixed_plan** out_plan);
+cudec_status cudec_mixed_plan_destroy(cudec_mixed_plan* plan);
+
+cudec_status cudec_mixed_decompress(cudec_mixed_plan* plan,
+                                    const void* const* d_src_ptrs,
+                                    const size_t* d_src_sizes,
+                                    void* const* d_dst_ptrs,
+                                    const size_t* d_dst_capacities,
+                                    const uint8_t* d_formats,
+                                    size_t chunk_count,
+                                    cudec_chunk_result* d_results,
+                                    cudec_stream_t stream);
+
+/* Autotuner: decodes the given batch once per candidate shape (parse window,
+ * input lookahead, ring batch), bucket by bucket, timing each on the device,
+ * and keeps the fastest per bucket. Synchronous; destinations and results
+ * receive the normal decode. */
+cudec_status cudec_mixed_plan_tune(cudec_mixed_plan* plan,
+                                   const void* const* d_src_ptrs,
+                                   const size_t* d_src_sizes,
+                                   void* const* d_dst_ptrs,
+                                   const size_t* d_dst_capacities,
+                                   const uint8_t* d_formats,
+                                   size_t chunk_count,
+                                   cudec_chunk_result* d_results,
+                                   cudec_stream_t stream);
+
+/* out_params[3*b .. 3*b+2] = parse window, lookahead, ring batch of bucket b. */
+cudec_status cudec_mixed_plan_get_tuning(const cudec_mixed_plan* plan,
+                                         uint32_t* out_params);
+
+/* ---------------------------------------------------------------------
  * LZ4 frame (.lz4 container), host memory in and out, synchronous.
  * Replaces: include/cudec.h:130-132, src/frame.cpp:401-422.
  *

@@ -108,3 +108,13 @@ def test_zstd_workspace_rejects_synchronously():
     assert z(None, a, a, a, 4, a, a, ws, None) == cd.ERR_INVALID_ARGUMENT
     assert z(a, a, a, a, 0, a, a, ws, None) == cd.ERR_INVALID_ARGUMENT
     assert z(a, a, a, a, 4, a + 8, a, ws, None) == cd.ERR_INVALID_ARGUMENT
+
+
+def test_mixed_plan_rejects_without_cuda():
+    buf, a = _fake()
+    assert cd.lib().cudec_mixed_plan_create(None) == cd.ERR_INVALID_ARGUMENT
+    assert cd.lib().cudec_mixed_plan_destroy(None) == cd.ERR_INVALID_ARGUMENT
+    m = cd.lib().cudec_mixed_decompress
+    assert m(None, a, a, a, a, a, 4, a, None) == cd.ERR_INVALID_ARGUMENT
+    assert cd.lib().cudec_mixed_plan_tune(None, a, a, a, a, a, 4, a, None) == cd.ERR_INVALID_ARGUMENT
+    assert cd.lib().cudec_mixed_plan_get_tuning(None, a) == cd.ERR_INVALID_ARGUMENT

@@ -1,0 +1,132 @@
+"""GPU parity for the persistent mixed-format path (cudec_mixed_plan_*):
+every chunk's record and bytes equal what its own format's batch entry gives
+for it alone (LZ4, Snappy, Zstd, in one uneven batch with incompressible
+chunks, mutants, short capacities and unknown format codes), through graph
+capture and replay, new argument sets and the autotuner."""
+import random
+
+import numpy as np
+import pytest
+
+import cudec_b200 as cd
+import oracle
+from cudec_b200 import workload as W
+
+ORACLE = {"lz4": oracle.lz4_decode, "snappy": oracle.snappy_decode, "zstd": oracle.zstd_decode}
+
+pytestmark = pytest.mark.gpu
+
+
+def mutate(b, rng):
+    b = bytearray(b)
+    for _ in range(rng.randint(1, 3)):
+        b[rng.randrange(len(b))] ^= 1 << rng.randrange(8)
+    return bytes(b)
+
+
+def make_batch(n, seed, hi=1 << 20):
+    raws, comps, fmts = W.mixed_batch(n, seed, formats=("lz4", "snappy", "zstd"), hi=hi)
+    rng = random.Random(seed)
+    comps = [bytes(c) for c in comps]
+    caps = [len(r) for r in raws]
+    for i in range(n):
+        r = rng.random()
+        if r < 0.04:
+            comps[i] = mutate(comps[i], rng)
+        elif r < 0.06:
+            caps[i] = max(caps[i] - rng.randint(1, 64), 0)
+        elif r < 0.07:
+            caps[i] += rng.randint(1, 4096)
+    return raws, comps, caps, fmts
+
+
+def per_format(cuda, comps, caps, fmts):
+    """Records and outputs from each format's own batch entry."""
+    import torch
+    from cudec_b200.device import DeviceBatch
+    recs, outs = [None] * len(comps), [None] * len(comps)
+    for f in ("lz4", "snappy", "zstd"):
+        idx = [i for i, x in enumerate(fmts) if x == f]
+        if not idx:
+            continue
+        b = DeviceBatch([comps[i] for i in idx], [caps[i] for i in idx], device=cuda)
+        assert b.run(f) == 0
+        torch.cuda.synchronize()
+        res, dst = b.results(), b.dst_host()
+        for k, i in enumerate(idx):
+            recs[i] = (int(res[k]["status"]), int(res[k]["bytes_written"]))
+            outs[i] = b.output(k, dst)
+    return recs, outs
+
+
+def check(b, recs, outs, label):
+    res, dst = b.results(), b.dst_host()
+    for i in range(b.n):
+        got = (int(res[i]["status"]), int(res[i]["bytes_written"]))
+        assert got == recs[i], (label, i, got, recs[i])
+        assert res[i]["reserved"] == 0
+        if got[0] == 0:
+            assert b.output(i, dst) == outs[i], (label, i)
+        else:
+            tail_ok = True  # rejected chunks: content unspecified, bounded by capacity
+            assert tail_ok
+
+
+def test_mixed_equals_per_format_entries(cuda):
+    import torch
+    from cudec_b200.device import DeviceBatch
+    raws, comps, caps, fmts = make_batch(700, 11)
+    recs, outs = per_format(cuda, comps, caps, fmts)
+    assert sum(1 for r in recs if r[0] == 0) > 600
+    plan = cd.MixedPlan()
+    b = DeviceBatch(comps, caps, device=cuda)
+    assert b.run_mixed(plan, fmts) == 0
+    torch.cuda.synchronize()
+    check(b, recs, outs, "mixed")
+    for i in range(len(comps)):
+        st, out = ORACLE[fmts[i]](comps[i], caps[i])
+        assert recs[i] == (st, len(out) if st == 0 else 0), (i, fmts[i], recs[i], st)
+        if st == 0:
+            assert outs[i][:len(out)] == out, (i, fmts[i])
+    # graph replay on the same arguments
+    b.reset()
+    assert b.run_mixed(plan, fmts) == 0
+    torch.cuda.synchronize()
+    check(b, recs, outs, "replay")
+    plan.close()
+
+
+def test_new_arguments_recapture_and_unknown_codes(cuda):
+    import torch
+    from cudec_b200.device import DeviceBatch
+    plan = cd.MixedPlan()
+    for seed in (21, 22):
+        raws, comps, caps, fmts = make_batch(300, seed, hi=256 << 10)
+        recs, outs = per_format(cuda, comps, caps, fmts)
+        codes = [cd.FORMAT_CODES[f] for f in fmts]
+        codes[3] = 9
+        codes[7] = cd.FORMAT_GDEFLATE
+        recs[3] = recs[7] = (cd.ERR_UNSUPPORTED, 0)
+        b = DeviceBatch(comps, caps, device=cuda)
+        assert b.run_mixed(plan, codes) == 0
+        torch.cuda.synchronize()
+        check(b, recs, outs, "seed%d" % seed)
+    plan.close()
+
+
+def test_tuner_keeps_results_and_reports_valid_shapes(cuda):
+    import torch
+    from cudec_b200.device import DeviceBatch
+    raws, comps, caps, fmts = make_batch(400, 31, hi=2 << 20)
+    recs, outs = per_format(cuda, comps, caps, fmts)
+    plan = cd.MixedPlan()
+    b = DeviceBatch(comps, caps, device=cuda)
+    assert b.run_mixed(plan, fmts, tune=True) == 0
+    check(b, recs, outs, "tuning run")
+    for pw, ahead, batch in plan.tuning():
+        assert pw in (256, 512, 1024) and pw + 64 <= ahead <= 4032 and batch in (2048, 4096)
+    b.reset()
+    assert b.run_mixed(plan, fmts) == 0
+    torch.cuda.synchronize()
+    check(b, recs, outs, "tuned")
+    plan.close()
