@@ -28,6 +28,14 @@ the launch itself is bracketed by CUDA events on its stream.
             uniform 0.2-0.8 per chunk, 5 % incompressible chunks, half LZ4 and
             half Snappy; the persistent work-stealing plan (tuned once, CUDA
             graph) against the plain path (one batch launch per format)
+  serve     the served mixed-format stream: Poisson arrivals, each request
+            1-4,096 chunks (log-uniform), 40 % LZ4 / 20 % Snappy / 30 % Zstd
+            level 3 (the 10 % GDeflate share is left out until that decoder
+            exists), sizes lognormal (median 32 KiB, sigma 1.0, 512 B -
+            2 MiB), a 32 GiB device budget, outputs kept on the device; p50 /
+            p99 latency and aggregate GB/s of the continuous-batching server
+            against the plain path (one request at a time, one launch per
+            format)
   per_format    the same measurement for raw Snappy (same content) and for
             Zstd: 4,096 frames of 1 MiB (1 MiB window, 128 KiB blocks, 10%
             repeated-byte runs, back-references up to 1 MiB), libzstd level 3
@@ -72,6 +80,10 @@ def parse_args():
                          "counts are for profiler captures)")
     ap.add_argument("--mixed-chunks", type=int, default=100000,
                     help="chunks of the uneven mixed LZ4+Snappy batch (0 skips it)")
+    ap.add_argument("--serve-requests", type=int, default=160,
+                    help="requests of the served mixed-format stream (0 skips it)")
+    ap.add_argument("--serve-rate", type=float, default=200.0,
+                    help="Poisson arrival rate of the served stream (requests/s)")
     ap.add_argument("--zstd-frames", type=int, default=4096,
                     help="Zstd frames per batch (0 skips the Zstd legs)")
     ap.add_argument("--zstd-unique", type=int, default=128,
@@ -317,6 +329,92 @@ def run_mixed(torch, cd, DeviceBatch, args, dev, stream, flush, max_over_ranks, 
     }
 
 
+SERVE_SEED = 0xC0DEC5
+SERVE_SLOTS = 32
+
+
+def serve_requests(k):
+    """The served stream's requests (seeded): packed input + per-chunk arrays."""
+    from cudec_b200 import workload as W
+    rng = np.random.default_rng(SERVE_SEED)
+    counts = np.rint(np.exp(rng.uniform(0, np.log(4096), k))).astype(int)
+    reqs = []
+    for i, n in enumerate(counts):
+        raws, comps, fmts = W.mixed_batch(int(n), SERVE_SEED * 7919 + i,
+                                          formats=("lz4", "snappy", "zstd"), weights=(4, 2, 3),
+                                          median=32768, sigma=1.0, lo=512, hi=2 << 20)
+        sizes = np.array([len(c) for c in comps], dtype=np.uint64)
+        offs = np.zeros(len(sizes), dtype=np.uint64)
+        offs[1:] = np.cumsum(sizes[:-1])
+        packed = np.frombuffer(b"".join(bytes(c) for c in comps), dtype=np.uint8)
+        import torch
+        pinned = torch.empty(len(packed), dtype=torch.uint8).pin_memory()
+        pinned.numpy()[:] = packed
+        reqs.append(dict(packed=pinned.numpy(), pin=pinned, offs=offs, sizes=sizes,
+                         caps=[len(r) for r in raws], fmts=fmts,
+                         check=(raws[0].tobytes(), raws[-1].tobytes())))
+    return reqs
+
+
+def serve_once(cd, reqs, mode, slots, rate):
+    """Replay the stream at `rate` requests/s into a fresh server."""
+    import threading
+    from cudec_b200.device import read_device
+    srv = cd.Server(32 << 30, max_inflight=slots, mode=mode, max_chunks=4096)
+    arrivals = np.cumsum(np.random.default_rng(SERVE_SEED + 1).exponential(1.0 / rate,
+                                                                            len(reqs)))
+    tickets = [None] * len(reqs)
+    late = []
+    t0 = time.perf_counter() + 0.05
+
+    def submitter():
+        for i, r in enumerate(reqs):
+            wait = t0 + arrivals[i] - time.perf_counter()
+            if wait > 0:
+                time.sleep(wait)
+            late.append(max(0.0, time.perf_counter() - (t0 + arrivals[i])))
+            st, t = srv.submit(r["packed"], r["offs"], r["sizes"], r["caps"], r["fmts"])
+            assert st == 0, st
+            tickets[i] = t
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    lats, t_end = [], 0.0
+    for i, r in enumerate(reqs):
+        while tickets[i] is None:
+            time.sleep(0.0002)
+        st, recs, ptrs, lat = srv.wait(tickets[i])
+        assert st == 0 and (recs["status"] == 0).all()
+        assert read_device(int(ptrs[0]), r["caps"][0]) == r["check"][0]
+        assert read_device(int(ptrs[-1]), r["caps"][-1]) == r["check"][1]
+        lats.append(lat)
+        t_end = time.perf_counter()
+        srv.release(tickets[i])
+    th.join()
+    srv.close()
+    total = float(sum(sum(r["caps"]) for r in reqs))
+    return {"p50_ms": round(float(np.percentile(lats, 50)), 3),
+            "p99_ms": round(float(np.percentile(lats, 99)), 3),
+            "mean_ms": round(float(np.mean(lats)), 3),
+            "value": round(total / (t_end - t0) / 1e9, 3),
+            "unit": "GB/s", "submit_late_p99_ms": round(1e3 * float(np.percentile(late, 99)), 3)}
+
+
+def run_serve(cd, args, dev):
+    reqs = serve_requests(args.serve_requests)
+    total = float(sum(sum(r["caps"]) for r in reqs))
+    mixed = serve_once(cd, reqs, cd.SERVER_MIXED, SERVE_SLOTS, args.serve_rate)
+    plain = serve_once(cd, reqs, cd.SERVER_PLAIN, 1, args.serve_rate)
+    return {"continuous_batching": mixed, "plain_queue": plain,
+            "requests": len(reqs), "rate_per_s": args.serve_rate,
+            "chunks": int(sum(len(r["caps"]) for r in reqs)),
+            "decompressed_bytes": int(total),
+            "offered_GBps": round(total / len(reqs) * args.serve_rate / 1e9, 3),
+            "budget_bytes": 32 << 30, "slots": SERVE_SLOTS,
+            "formats": "40 % LZ4 / 20 % Snappy / 30 % Zstd L3 (GDeflate share not yet served)",
+            "latency": "submit to completion, measured by the server"}
+
+
 def time_device(torch, batch, fmt, stream, flush, steps, warmup):
     """Mean launch time (ms) of the batch entry, L2 flushed before each."""
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
@@ -410,6 +508,11 @@ def main():
         mixed_line = run_mixed(torch, cd, DeviceBatch, args, dev, stream, flush,
                                max_over_ranks, world, warm)
 
+    # ---- served stream: continuous batching vs the plain queue --------
+    serve_line = None
+    if args.serve_requests > 0:
+        serve_line = run_serve(cd, args, dev)
+
     # ---- Zstd, 1 MiB frames at levels 3 and 19 ------------------------
     zstd_lines = {}
     if args.zstd_frames > 0:
@@ -502,6 +605,7 @@ def main():
                 **zstd_lines,
             },
             **({"mixed": mixed_line} if mixed_line else {}),
+            **({"serve": serve_line} if serve_line else {}),
             "gpu_launches": args.steps,
             "clocks": clocks.summary(),
         }

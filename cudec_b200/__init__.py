@@ -60,6 +60,11 @@ SIGNATURES = {
     "cudec_mixed_decompress": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _SZ, _P, _P]),
     "cudec_mixed_plan_tune": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _SZ, _P, _P]),
     "cudec_mixed_plan_get_tuning": (ctypes.c_int, [_P, _P]),
+    "cudec_server_create": (ctypes.c_int, [_SZ, ctypes.c_int, ctypes.c_int, _SZ, _P]),
+    "cudec_server_destroy": (ctypes.c_int, [_P]),
+    "cudec_server_submit": (ctypes.c_int, [_P, _P, _SZ, _P, _P, _P, _P, _SZ, _P]),
+    "cudec_server_wait": (ctypes.c_int, [_P, ctypes.c_uint64, _P, _P, _P]),
+    "cudec_server_release": (ctypes.c_int, [_P, ctypes.c_uint64]),
     "cudec_lz4f_decompress": (ctypes.c_int, [_P, _SZ, _P, _SZ, _P]),
     "cudec_stream_ctx_create": (ctypes.c_int, [_P]),
     "cudec_lz4_decompress_stream_ctx": (ctypes.c_int, [_P, _P, _P, _P, _P, _SZ, ctypes.c_int, _P]),
@@ -215,6 +220,69 @@ class MixedPlan:
         if self.handle:
             lib().cudec_mixed_plan_destroy(self.handle)
             self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+SERVER_MIXED, SERVER_PLAIN = 0, 1
+
+
+class Server:
+    """cudec_server: continuous-batching decode with a device-memory budget."""
+
+    def __init__(self, budget_bytes, max_inflight=4, mode=SERVER_MIXED, max_chunks=4096):
+        h = ctypes.c_void_p()
+        st = lib().cudec_server_create(budget_bytes, max_inflight, mode, max_chunks,
+                                       ctypes.byref(h))
+        if st != OK:
+            raise RuntimeError("cudec_server_create: %s" % STATUS_NAMES.get(st, st))
+        self.handle = h
+        self._keep = {}
+
+    def submit(self, packed, offsets, sizes, caps, formats):
+        """packed: numpy uint8 array (kept alive until wait); the per-chunk
+        arrays are sequences of ints / format codes. Returns (status, ticket)."""
+        import numpy as np
+        offs = np.ascontiguousarray(offsets, dtype=np.uint64)
+        szs = np.ascontiguousarray(sizes, dtype=np.uint64)
+        cps = np.ascontiguousarray(caps, dtype=np.uint64)
+        fms = np.ascontiguousarray([FORMAT_CODES.get(f, f) if isinstance(f, str) else f
+                                    for f in formats], dtype=np.uint8)
+        t = ctypes.c_uint64()
+        st = lib().cudec_server_submit(self.handle, packed.ctypes.data if len(packed) else None,
+                                       len(packed), offs.ctypes.data, szs.ctypes.data,
+                                       cps.ctypes.data, fms.ctypes.data, len(offs),
+                                       ctypes.byref(t))
+        if st == OK:
+            self._keep[t.value] = (packed, len(offs))
+        return st, t.value
+
+    def wait(self, ticket):
+        """Returns (status, records, device output addresses, latency_ms)."""
+        import numpy as np
+        n = self._keep[ticket][1]
+        recs = np.zeros(n, dtype=[("status", "<i4"), ("reserved", "<u4"),
+                                  ("bytes_written", "<u8")])
+        ptrs = np.zeros(n, dtype=np.uint64)
+        lat = ctypes.c_double()
+        st = lib().cudec_server_wait(self.handle, ticket, recs.ctypes.data, ptrs.ctypes.data,
+                                     ctypes.byref(lat))
+        return st, recs, ptrs, lat.value
+
+    def release(self, ticket):
+        st = lib().cudec_server_release(self.handle, ticket)
+        self._keep.pop(ticket, None)
+        return st
+
+    def close(self):
+        if self.handle:
+            lib().cudec_server_destroy(self.handle)
+            self.handle = None
+            self._keep.clear()
 
     def __del__(self):
         try:

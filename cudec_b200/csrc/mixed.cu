@@ -31,6 +31,7 @@
 #include "host_util.h"
 #include "launch.h"
 #include "lz_warp_kernel.cuh"
+#include "mixed.h"
 #include "zstd_frame.cuh"
 
 namespace cdb {
@@ -229,7 +230,9 @@ Args make_args(cudec_mixed_plan* p, const Key& k) {
     return a;
 }
 
-// The whole decode of one batch on stream s: order, then the persistent grid.
+// The whole decode of one batch on stream s: order, then the persistent grid
+// (no more CTAs than the batch has chunks for, so small batches leave SMs to
+// other work on the device).
 cudaError_t enqueue(cudec_mixed_plan* p, const Key& k, cudaStream_t s) {
     Ctrl* ctrl = static_cast<Ctrl*>(p->ctrl.p);
     cudaError_t e = cudaMemsetAsync(ctrl, 0, sizeof(Ctrl), s);
@@ -240,7 +243,9 @@ cudaError_t enqueue(cudec_mixed_plan* p, const Key& k, cudaStream_t s) {
     cdb::mixed::order_scan<<<1, 32, 0, s>>>(ctrl);
     cdb::mixed::order_place<<<blocks, 256, 0, s>>>(k.caps, k.n, ctrl,
                                                     static_cast<uint32_t*>(p->order.p));
-    cdb::mixed::mixed_kernel<<<p->grid, cdb::mixed::kThreads, cdb::mixed::kSmem, s>>>(
+    const size_t ctas = (k.n + cdb::mixed::kWarps - 1) / cdb::mixed::kWarps;
+    const unsigned grid = static_cast<unsigned>(std::min<size_t>(ctas, p->grid));
+    cdb::mixed::mixed_kernel<<<grid, cdb::mixed::kThreads, cdb::mixed::kSmem, s>>>(
         make_args(p, k));
     return cudaGetLastError();
 }
@@ -257,6 +262,26 @@ cudec_status bind(cudec_mixed_plan* p, size_t n) {
 }
 
 }  // namespace
+
+namespace cdb {
+
+cudaError_t mixed_reserve(cudec_mixed_plan* plan, size_t max_chunks) {
+    if (plan->order.cap >= max_chunks * sizeof(uint32_t)) return cudaSuccess;
+    plan->drop_graph();
+    return plan->order.ensure(max_chunks * sizeof(uint32_t));
+}
+
+cudaError_t mixed_launch(cudec_mixed_plan* plan, const void* const* d_src_ptrs,
+                         const size_t* d_src_sizes, void* const* d_dst_ptrs,
+                         const size_t* d_dst_capacities, const uint8_t* d_formats, size_t n,
+                         cudec_chunk_result* d_results, cudaStream_t stream) {
+    if (plan->order.cap < n * sizeof(uint32_t)) return cudaErrorInvalidValue;
+    return enqueue(plan, Key{d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_capacities, d_formats, n,
+                             d_results},
+                   stream);
+}
+
+}  // namespace cdb
 
 extern "C" {
 

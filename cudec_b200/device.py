@@ -110,3 +110,18 @@ class DeviceBatch:
         o = int(self.dst_offs[i])
         n = int(self.caps[i]) if length is None else length
         return dst[o:o + n].tobytes()
+
+
+class _DevView:
+    """A raw device byte range, viewable by torch without a copy."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": "|u1",
+                                         "data": (int(ptr), False), "version": 3}
+
+
+def read_device(ptr, n, device="cuda"):
+    """Copy n bytes at device address ptr to host bytes."""
+    if n == 0:
+        return b""
+    return torch.as_tensor(_DevView(ptr, n), device=device).cpu().numpy().tobytes()

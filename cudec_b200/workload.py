@@ -258,16 +258,20 @@ def mixed_sizes(n, seed, median=16384, sigma=1.2, lo=256, hi=4 << 20):
 
 
 def mixed_batch(n, seed, formats=("lz4", "snappy"), median=16384, sigma=1.2, lo=256,
-                hi=4 << 20, random_frac=0.05, threads=None):
+                hi=4 << 20, random_frac=0.05, threads=None, weights=None, zstd_level=3):
     """The uneven mixed batch: lognormal sizes, copy probability uniform in
     0.2-0.8 per chunk, `random_frac` of the chunks uniform random bytes, the
-    format of chunk i = formats[i % len(formats)]. Returns (raws, comps, fmts)
-    with raws as numpy views of one buffer."""
+    format of chunk i = formats[i % len(formats)], or drawn with `weights`.
+    Returns (raws, comps, fmts) with raws as numpy views of one buffer."""
     sizes = mixed_sizes(n, seed, median, sigma, lo, hi)
     rng = np.random.default_rng(seed + 1)
     probs = rng.uniform(0.2, 0.8, n)
     rand = rng.random(n) < random_frac
-    fmts = [formats[i % len(formats)] for i in range(n)]
+    if weights is None:
+        fmts = [formats[i % len(formats)] for i in range(n)]
+    else:
+        w = np.asarray(weights, dtype=np.float64)
+        fmts = [formats[k] for k in rng.choice(len(formats), size=n, p=w / w.sum())]
     params = [(zstd_params(float(p), 0.1) if f == "zstd" else lz_params(float(p), bool(r)))
               for p, r, f in zip(probs, rand, fmts)]
     for i, f in enumerate(fmts):
@@ -276,12 +280,18 @@ def mixed_batch(n, seed, formats=("lz4", "snappy"), median=16384, sigma=1.2, lo=
     seeds = np.array([chunk_seed(seed, 2, i) for i in range(n)], dtype=np.uint64)
     buf, offs = generate(sizes, params, param_idx=np.arange(n), seeds=seeds, threads=threads)
     raws = [buf[int(o):int(o) + int(s)] for o, s in zip(offs, sizes)]
-    comps = []
-    for r, f in zip(raws, fmts):
+    def one(k):
+        r, f = raws[k], fmts[k]
         if f == "lz4":
-            comps.append(lz4_compress(r))
-        elif f == "snappy":
-            comps.append(snappy_compress(r))
-        else:
-            comps.append(zstd_compress(r.tobytes(), 3, 20, True))
+            return lz4_compress(r)
+        if f == "snappy":
+            return snappy_compress(r)
+        return zstd_compress(r.tobytes(), zstd_level, 20, True)
+
+    if n >= 256:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(max_workers=min(os.cpu_count() or 1, 32)) as ex:
+            comps = list(ex.map(one, range(n), chunksize=64))
+    else:
+        comps = [one(k) for k in range(n)]
     return raws, comps, fmts

@@ -213,6 +213,45 @@ cudec_status cudec_mixed_plan_get_tuning(const cudec_mixed_plan* plan,
                                          uint32_t* out_params);
 
 /* ---------------------------------------------------------------------
+ * Continuous-batching decode server (no counterpart in the reference). A
+ * server owns a device arena of `device_budget_bytes` and `max_inflight`
+ * slots (a stream and a mixed plan each). Requests are admitted in arrival
+ * order as soon as a slot and enough of the budget are free, so requests
+ * that arrive while others run overlap with them on the device. A request's
+ * footprint (tables, compressed input, 16-byte-aligned outputs) must fit the
+ * whole budget. Outputs stay in the arena until the request is released.
+ * CUDEC_SERVER_PLAIN (requires max_inflight == 1) decodes each request with
+ * the per-format batch entries in arrival order: the comparison path. */
+#define CUDEC_SERVER_MIXED 0
+#define CUDEC_SERVER_PLAIN 1
+
+typedef struct cudec_server cudec_server;
+
+cudec_status cudec_server_create(size_t device_budget_bytes, int max_inflight, int mode,
+                                 size_t max_chunks_per_request, cudec_server** out_server);
+/* Waits for admitted work; requests still queued are decoded first. */
+cudec_status cudec_server_destroy(cudec_server* server);
+
+/* h_input holds the compressed chunks (chunk i at h_offsets[i], h_sizes[i]
+ * bytes) and must stay valid until cudec_server_wait returns for the ticket;
+ * the per-chunk arrays are copied. Returns at once with a ticket. */
+cudec_status cudec_server_submit(cudec_server* server, const void* h_input, size_t input_bytes,
+                                 const size_t* h_offsets, const size_t* h_sizes,
+                                 const size_t* h_dst_caps, const uint8_t* h_formats,
+                                 size_t chunk_count, uint64_t* out_ticket);
+
+/* Blocks until the request is decoded. h_results (chunk_count records) and
+ * h_dst_ptrs (device addresses of the outputs) may be NULL; *out_latency_ms =
+ * submit to completion. Returns CUDEC_ERR_CUDA if the request's device work
+ * failed, else CUDEC_OK (per-chunk statuses in the records). */
+cudec_status cudec_server_wait(cudec_server* server, uint64_t ticket,
+                               cudec_chunk_result* h_results, void** h_dst_ptrs,
+                               double* out_latency_ms);
+
+/* Returns the request's device memory to the budget (after wait). */
+cudec_status cudec_server_release(cudec_server* server, uint64_t ticket);
+
+/* ---------------------------------------------------------------------
  * LZ4 frame (.lz4 container), host memory in and out, synchronous.
  * Replaces: include/cudec.h:130-132, src/frame.cpp:401-422.
  *

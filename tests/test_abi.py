@@ -118,3 +118,21 @@ def test_mixed_plan_rejects_without_cuda():
     assert m(None, a, a, a, a, a, 4, a, None) == cd.ERR_INVALID_ARGUMENT
     assert cd.lib().cudec_mixed_plan_tune(None, a, a, a, a, a, 4, a, None) == cd.ERR_INVALID_ARGUMENT
     assert cd.lib().cudec_mixed_plan_get_tuning(None, a) == cd.ERR_INVALID_ARGUMENT
+
+
+def test_server_rejects_without_cuda():
+    buf, a = _fake()
+    h = ctypes.c_void_p()
+    c = cd.lib().cudec_server_create
+    assert c(0, 4, cd.SERVER_MIXED, 4096, ctypes.byref(h)) == cd.ERR_INVALID_ARGUMENT
+    assert c(1 << 20, 0, cd.SERVER_MIXED, 4096, ctypes.byref(h)) == cd.ERR_INVALID_ARGUMENT
+    assert c(1 << 20, 2, cd.SERVER_PLAIN, 4096, ctypes.byref(h)) == cd.ERR_INVALID_ARGUMENT
+    assert c(1 << 20, 4, 7, 4096, ctypes.byref(h)) == cd.ERR_INVALID_ARGUMENT
+    assert c(1 << 20, 4, cd.SERVER_MIXED, 0, ctypes.byref(h)) == cd.ERR_INVALID_ARGUMENT
+    assert c(1 << 20, 4, cd.SERVER_MIXED, 4096, None) == cd.ERR_INVALID_ARGUMENT
+    t = ctypes.c_uint64()
+    assert cd.lib().cudec_server_submit(None, a, 8, a, a, a, a, 1, ctypes.byref(t)) == \
+        cd.ERR_INVALID_ARGUMENT
+    assert cd.lib().cudec_server_wait(None, 1, None, None, None) == cd.ERR_INVALID_ARGUMENT
+    assert cd.lib().cudec_server_release(None, 1) == cd.ERR_INVALID_ARGUMENT
+    assert cd.lib().cudec_server_destroy(None) == cd.ERR_INVALID_ARGUMENT
