@@ -72,10 +72,10 @@ def build(verbose=False, extra_nvcc=()):
     if _stale(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs +
              ["-lpthread", "-ldl", "-lrt"], verbose)
-    wsrc = os.path.join(CSRC, "workload.c")
-    if _stale(WORKLOAD, [wsrc]):
+    wsrc = [os.path.join(CSRC, "workload.c"), os.path.join(CSRC, "gdeflate_enc.c")]
+    if _stale(WORKLOAD, wsrc):
         _run(["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-pthread", "-o",
-              WORKLOAD, wsrc, "-lm"], verbose)
+              WORKLOAD] + wsrc + ["-lm"], verbose)
     return LIB
 
 

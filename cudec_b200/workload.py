@@ -295,3 +295,44 @@ def mixed_batch(n, seed, formats=("lz4", "snappy"), median=16384, sigma=1.2, lo=
     else:
         comps = [one(k) for k in range(n)]
     return raws, comps, fmts
+
+
+def gdeflate_params(copy_prob=0.5):
+    """GDeflate content: the generator with a 256-symbol Zipf(1.3) alphabet,
+    matches of 3-258 bytes and offsets up to 32 KiB."""
+    return GenParams(copy_prob, 256, 1.3, 8.0, 16.0, 3, 258, 32768, 0.0, 1.0, 0)
+
+
+def _gd():
+    lib = _wlib()
+    if not getattr(lib, "_gd_ready", False):
+        for name in ("gdeflate_compress_page", "gdeflate_compress_tilestream"):
+            f = getattr(lib, name)
+            f.restype = ctypes.c_size_t
+            f.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
+                          ctypes.c_int, ctypes.c_uint32]
+        lib._gd_ready = True
+    return lib
+
+
+def gdeflate_compress(data, level=12, window=32768):
+    """One GDeflate page (len(data) <= 65536) from the build's own encoder."""
+    data = bytes(data)
+    assert len(data) <= 65536
+    cap = 2 * len(data) + 4096
+    out = ctypes.create_string_buffer(cap)
+    n = _gd().gdeflate_compress_page(data, len(data), out, cap, level, window)
+    if n == 0:
+        raise RuntimeError("gdeflate_compress_page failed")
+    return out.raw[:n]
+
+
+def gdeflate_tilestream(data, level=12, window=32768):
+    """A TileStream container of 64 KiB GDeflate pages."""
+    data = bytes(data)
+    cap = 2 * len(data) + 8192 + 8 * (len(data) // 65536 + 1)
+    out = ctypes.create_string_buffer(cap)
+    n = _gd().gdeflate_compress_tilestream(data, len(data), out, cap, level, window)
+    if n == 0:
+        raise RuntimeError("gdeflate_compress_tilestream failed")
+    return out.raw[:n]

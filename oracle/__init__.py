@@ -1,8 +1,9 @@
 """ORACLE — test infrastructure, not part of the product.
 
 ctypes loaders for:
-  liboracle.so          the C restatement of the reference ladders (oracle.c)
-                        and the multithreaded codec-library harness (codecs.c)
+  liboracle.so          the C restatements of the reference ladders (oracle.c,
+                        zstd_oracle.c, gdeflate_oracle.c) and the
+                        multithreaded codec-library harness (codecs.c)
   _ref/libref_twin.so   the reference's own host twins, compiled in place
   _ref/libcudec_ref.so  the reference library (GPU), compiled in place
 
@@ -61,6 +62,9 @@ def oracle_lib():
         "codec_decode_batch": (ctypes.c_int, [ctypes.c_int] + _BATCH),
         "codec_lz4_version": (ctypes.c_int, []),
         "codec_zstd_version": (ctypes.c_int, []),
+        "oracle_gdeflate_decode": (ctypes.c_int, _DEC),
+        "oracle_gdeflate_schedule_trace": (ctypes.c_int, [_U8P, _U64, _U8P, _U64, _U8P]),
+        "oracle_tilestream_parse": (ctypes.c_int, [_U8P, _U64, _U8P, _U64, _U8P, _U8P]),
     })
     if h is None:
         raise RuntimeError("oracle/liboracle.so is not built (oracle.build())")
@@ -76,6 +80,8 @@ def ref_twin_lib():
         "ref_zstd_twin_decode_batch": (ctypes.c_int, _BATCH),
         "ref_lz4_twin_decode_batch": (ctypes.c_int, _BATCH),
         "ref_snappy_twin_decode_batch": (ctypes.c_int, _BATCH),
+        "ref_gdeflate_schedule_trace": (ctypes.c_int, [_U8P, _U64, _U8P, _U64, _U8P]),
+        "ref_tilestream_parse": (ctypes.c_int, [_U8P, _U64, _U8P, _U64, _U8P, _U8P]),
     })
 
 
@@ -135,6 +141,48 @@ def ref_zstd_decode(frame, cap):
     """(status, bytes) from the reference's twin driver, or None if unbuilt."""
     h = ref_twin_lib()
     return None if h is None else _decode_one(h.ref_zstd_twin_decode, frame, cap)
+
+
+def gdeflate_decode(page, cap):
+    """One GDeflate page (oracle/gdeflate_oracle.c; symbol-level parity with the
+    GDeflate reference decoder is unpinned)."""
+    return _decode_one(oracle_lib().oracle_gdeflate_decode, page, cap)
+
+
+def _schedule_trace(fn, page, ops):
+    ops = np.ascontiguousarray(ops, dtype=np.uint32)
+    buf = np.frombuffer(bytes(page) + b"\0", dtype=np.uint8)
+    trace = np.zeros(4 * (len(ops) + 1), dtype=np.uint64)
+    n = fn(buf.ctypes.data, len(page), ops.ctypes.data, len(ops), trace.ctypes.data)
+    return trace[:4 * n].reshape(-1, 4)
+
+
+def gdeflate_schedule_trace(page, ops):
+    return _schedule_trace(oracle_lib().oracle_gdeflate_schedule_trace, page, ops)
+
+
+def ref_gdeflate_schedule_trace(page, ops):
+    return _schedule_trace(ref_twin_lib().ref_gdeflate_schedule_trace, page, ops)
+
+
+def _tilestream(fn, stream, tiles_cap):
+    buf = np.frombuffer(bytes(stream) + b"\0", dtype=np.uint8)
+    tiles = np.zeros(3 * max(tiles_cap, 1), dtype=np.uint64)
+    cnt, tot = _U64(), _U64()
+    st = fn(buf.ctypes.data, len(stream), tiles.ctypes.data, tiles_cap, ctypes.byref(cnt),
+            ctypes.byref(tot))
+    if st != 0:
+        return st, None, None
+    return st, tiles[:3 * cnt.value].reshape(-1, 3).tolist(), tot.value
+
+
+def tilestream_parse(stream, tiles_cap):
+    """(status, [[src_off, src_size, dst_size], ...], total) of the envelope."""
+    return _tilestream(oracle_lib().oracle_tilestream_parse, stream, tiles_cap)
+
+
+def ref_tilestream_parse(stream, tiles_cap):
+    return _tilestream(ref_twin_lib().ref_tilestream_parse, stream, tiles_cap)
 
 
 def snappy_decode(comp, cap):

@@ -17,6 +17,8 @@
 #include "lz4_twin.h"
 #include "snappy_twin.h"
 #include "zstd_twin_driver.h"
+#include "gdeflate_schedule.h"
+#include "tilestream.h"
 
 #include <atomic>
 #include <cstdint>
@@ -106,6 +108,57 @@ int ref_snappy_twin_decode_batch(const uint8_t* const* src,
                                  int threads) {
     return ref_batch(ref_snappy_twin_decode, src, sizes, dst, caps, n, status,
                      written, threads);
+}
+
+
+// The reference's GDeflate refill schedule (src/gdeflate_schedule.h) run over
+// an operation list, recording the state after each op: the same encoding as
+// oracle_gdeflate_schedule_trace (0 advance, 1..64 pop, 100 reset, 200
+// ensure, 300 remove of the next slot's width).
+int ref_gdeflate_schedule_trace(const uint8_t* page, uint64_t bytes, const uint32_t* ops,
+                                uint64_t n_ops, uint64_t* trace) {
+    using namespace cudec_detail;
+    GDeflateSchedule s;
+    const bool ok = GDeflateInit(s, page, bytes);
+    trace[0] = s.cursor;
+    trace[1] = s.idx;
+    trace[2] = s.failed ? 1 : 0;
+    trace[3] = ok ? 1 : 0;
+    uint64_t t = 4, i = 0;
+    while (i < n_ops) {
+        const uint32_t op = ops[i++];
+        uint64_t v = 0;
+        if (op == 0) GDeflateAdvance(s, page);
+        else if (op <= 64) v = GDeflatePop(s, op);
+        else if (op == 100) GDeflateReset(s);
+        else if (op == 200) GDeflateEnsure(s, page);
+        else if (op == 300 && i < n_ops) GDeflateRemove(s, ops[i++]);
+        trace[t++] = s.cursor;
+        trace[t++] = s.idx;
+        trace[t++] = s.failed ? 1 : 0;
+        trace[t++] = v;
+    }
+    return static_cast<int>(t / 4);
+}
+
+// The reference's TileStream envelope walker (src/tilestream.h); tiles gets
+// three words per tile (src offset, src size, dst size).
+int ref_tilestream_parse(const uint8_t* st, uint64_t size, uint64_t* tiles, uint64_t tiles_cap,
+                         uint64_t* count, uint64_t* total) {
+    using namespace cudec_detail;
+    std::vector<TileStreamTile> t(tiles_cap ? tiles_cap : 1);
+    TileStreamInfo info{};
+    const cudec_status st_ = TileStreamParse(st, size, t.data(), tiles_cap, &info);
+    if (st_ == CUDEC_OK) {
+        for (uint64_t k = 0; k < info.tile_count; ++k) {
+            tiles[3 * k] = t[k].src_off;
+            tiles[3 * k + 1] = t[k].src_size;
+            tiles[3 * k + 2] = t[k].dst_size;
+        }
+        *count = info.tile_count;
+        *total = info.total_uncompressed;
+    }
+    return st_;
 }
 
 }  // extern "C"

@@ -145,6 +145,53 @@ def zstd_vectors():
     return out
 
 
+def tilestream_vectors():
+    """fuzz/corpus/fuzz_gdeflate_tilestream/* (framing per
+    fuzz/fuzz_gdeflate_tilestream.cpp: byte 0 selects the tile-array capacity
+    - odd: the declared count minus byte0 >> 1, floored at 0 - and the rest is
+    the stream); verdicts and tile tables from the reference's own walker
+    (src/tilestream.h, compiled into oracle/_ref/libref_twin.so)."""
+    out = []
+    d = os.path.join(REF, "fuzz", "corpus", "fuzz_gdeflate_tilestream")
+    for f in sorted(os.listdir(d)):
+        raw = open(os.path.join(d, f), "rb").read()
+        if not raw:
+            continue
+        sel, stream = raw[0], raw[1:1 + (1 << 13)]
+        declared = stream[2] | (stream[3] << 8) if len(stream) >= 4 else 0
+        cap = declared
+        if sel & 1:
+            cap = max(declared - (sel >> 1), 0)
+        st, tiles, total = oracle.ref_tilestream_parse(stream, cap)
+        out.append({"name": "seed/" + f, "input_hex": stream.hex(), "tiles_capacity": cap,
+                    "expect_status": st, "expect_tiles": tiles, "expect_total": total})
+    return out
+
+
+def gdeflate_vectors():
+    """Pages from this build's own encoder with their decoded digests. No
+    GDeflate reference decoder or vector exists in the reference tree, so
+    these pin the build's format decisions against later change; they are
+    not parity with the GDeflate reference."""
+    import numpy as np
+    out = []
+    sizes = [0, 1, 100, 4096, 65536, 65536]
+    buf, offs = workload.generate(sizes, [workload.gdeflate_params(0.5)],
+                                  seeds=np.arange(40, 40 + len(sizes), dtype=np.uint64))
+    raws = [buf[int(o):int(o) + n].tobytes() for o, n in zip(offs, sizes)]
+    raws += [bytes(range(256)) * 256, b"\x00" * 65536,
+             bytes(np.random.default_rng(3).integers(0, 256, 3000, dtype=np.uint8))]
+    for i, raw in enumerate(raws):
+        for lvl in (1, 12):
+            page = workload.gdeflate_compress(raw, lvl)
+            st, dec = oracle.gdeflate_decode(page, len(raw))
+            assert st == 0 and dec == raw
+            out.append({"name": "page/%d-%d-L%d" % (i, len(raw), lvl), "input_hex": page.hex(),
+                        "capacity": len(raw), "expect_status": 0, "expect_len": len(raw),
+                        "expect_sha256": hashlib.sha256(raw).hexdigest()})
+    return out
+
+
 def _declared(body):
     v = 0
     for k in range(5):
@@ -164,7 +211,9 @@ def main():
         sys.exit("oracle/_ref/libref_twin.so missing: run make -f oracle/Makefile")
     for name, vecs in (("lz4_block.json", lz4_vectors()),
                        ("snappy_block.json", snappy_vectors()),
-                       ("zstd_frame.json", zstd_vectors())):
+                       ("zstd_frame.json", zstd_vectors()),
+                       ("tilestream.json", tilestream_vectors()),
+                       ("gdeflate_page.json", gdeflate_vectors())):
         with open(os.path.join(OUT, name), "w") as f:
             json.dump({"generated_by": "tests/golden/make_golden.py",
                        "lz4_version": workload.lz4_version(),
