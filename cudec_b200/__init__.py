@@ -55,6 +55,9 @@ SIGNATURES = {
     "cudec_zstd_workspace_bytes": (ctypes.c_size_t, [_SZ]),
     "cudec_zstd_decompress_batch": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P, _SZ, _P]),
     "cudec_zstd_decompress_batch_noalloc": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P]),
+    "cudec_gdeflate_decompress_batch": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P]),
+    "cudec_gdeflate_tilestream_parse": (ctypes.c_int, [_P, _SZ, _P, _SZ, _P, _P]),
+    "cudec_gdeflate_tilestream_decompress": (ctypes.c_int, [_P, _SZ, _P, _SZ, ctypes.c_int, _P]),
     "cudec_mixed_plan_create": (ctypes.c_int, [_P]),
     "cudec_mixed_plan_destroy": (ctypes.c_int, [_P]),
     "cudec_mixed_decompress": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _SZ, _P, _P]),
@@ -136,9 +139,42 @@ def zstd_decompress_batch_noalloc(d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_cap
                                                      d_dst_caps, n, d_results, stream)
 
 
+def gdeflate_decompress_batch(d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_caps, n, d_results,
+                              stream=None):
+    """cudec_gdeflate_decompress_batch (one GDeflate page per chunk)."""
+    return lib().cudec_gdeflate_decompress_batch(d_src_ptrs, d_src_sizes, d_dst_ptrs,
+                                                 d_dst_caps, n, d_results, stream)
+
+
+def tilestream_parse(stream, tiles_capacity):
+    """(status, [(src_offset, src_size, dst_size)], total) from the library's
+    TileStream walker."""
+    import numpy as np
+    buf = bytes(stream)
+    tiles = np.zeros(3 * max(tiles_capacity, 1), dtype=np.uint64)
+    cnt, tot = ctypes.c_size_t(), ctypes.c_size_t()
+    st = lib().cudec_gdeflate_tilestream_parse(buf, len(buf), tiles.ctypes.data,
+                                               tiles_capacity, ctypes.byref(cnt),
+                                               ctypes.byref(tot))
+    if st != OK:
+        return st, None, None
+    return st, tiles[:3 * cnt.value].reshape(-1, 3).tolist(), tot.value
+
+
+def tilestream_decompress(stream, capacity):
+    """Whole container into host memory: (status, bytes)."""
+    buf = bytes(stream)
+    out = ctypes.create_string_buffer(max(capacity, 1))
+    written = ctypes.c_size_t()
+    st = lib().cudec_gdeflate_tilestream_decompress(buf, len(buf), out, capacity, MEM_HOST,
+                                                    ctypes.byref(written))
+    return st, out.raw[:written.value]
+
+
 BATCH_ENTRIES = {
     "lz4": lz4_decompress_batch,
     "snappy": snappy_decompress_batch,
+    "gdeflate": gdeflate_decompress_batch,
 }
 
 

@@ -31,7 +31,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-I" + INC, "-I" + CSRC,
              "-I/usr/local/cuda/include", "-Wall", "-Wextra"]
 CC_FLAGS = ["-O2", "-std=c11", "-fPIC", "-I" + INC, "-Wall", "-Wextra"]
 
-LIB_SOURCES = ["batch.cu", "zstd.cu", "mixed.cu", "serve.cpp", "frame.cpp", "stream.cpp", "host_util.cpp", "version.c"]
+LIB_SOURCES = ["batch.cu", "zstd.cu", "mixed.cu", "gdeflate.cu", "serve.cpp", "frame.cpp", "stream.cpp", "host_util.cpp", "version.c"]
 
 
 def _headers():

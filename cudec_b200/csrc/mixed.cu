@@ -1,7 +1,9 @@
 // Persistent mixed-format batch decode.
 //
-// One launch decodes a batch whose chunks are LZ4 blocks, raw Snappy blocks
-// and Zstd frames in any mix and of any sizes (a per-chunk format code). A
+// One launch decodes a batch whose chunks are LZ4 blocks, raw Snappy blocks,
+// Zstd frames and GDeflate pages in any mix and of any sizes (a per-chunk
+// format code; GDeflate pages are written straight to their destinations
+// here, the tables in the warp's shared memory). A
 // plan owns everything the launch needs so the call allocates nothing:
 //
 //   * a largest-first order of the chunks (by output capacity), built on the
@@ -30,6 +32,7 @@
 #include "cudec.h"
 #include "host_util.h"
 #include "launch.h"
+#include "gdeflate_page.cuh"
 #include "lz_warp_kernel.cuh"
 #include "mixed.h"
 #include "zstd_frame.cuh"
@@ -39,9 +42,10 @@ namespace mixed {
 
 constexpr uint32_t kWarps = 4;
 constexpr uint32_t kThreads = 32 * kWarps;
-constexpr uint32_t kWarpSmem = lzw::kWarpSmem > sizeof(zstd::WarpSmem)
-                                   ? lzw::kWarpSmem
-                                   : static_cast<uint32_t>(sizeof(zstd::WarpSmem));
+constexpr uint32_t kMaxOf(uint32_t a, uint32_t b) { return a > b ? a : b; }
+constexpr uint32_t kWarpSmem =
+    kMaxOf(kMaxOf(lzw::kWarpSmem, static_cast<uint32_t>(sizeof(zstd::WarpSmem))),
+           static_cast<uint32_t>(sizeof(gdf::Tables)));
 constexpr uint32_t kSmem = kWarps * kWarpSmem;
 constexpr int kBuckets = CUDEC_MIXED_BUCKETS;
 constexpr int kClasses = 64;  // floor(log2(capacity)) classes for the order
@@ -138,6 +142,11 @@ __global__ void __launch_bounds__(kThreads) mixed_kernel(Args a) {
                     src, S, dst, cap, base, base + lzw::kRing,
                     reinterpret_cast<uint16_t*>(base + lzw::kRing + lzw::kIn),
                     a.tune[size_bucket(cap)], lane, &written);
+                break;
+            case CUDEC_FORMAT_GDEFLATE:
+                st = gdf::decode_page<false>(src, S, dst, cap, nullptr,
+                                             *reinterpret_cast<gdf::Tables*>(base), lane,
+                                             &written);
                 break;
             case CUDEC_FORMAT_ZSTD:
                 st = zstd::decode_frame(src, S, dst, cap, *reinterpret_cast<zstd::WarpSmem*>(base),

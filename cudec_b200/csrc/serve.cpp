@@ -193,6 +193,9 @@ cudaError_t cudec_server::launch(Slot& sl, Request& r) {
             else if (fmts[j] == CUDEC_FORMAT_SNAPPY)
                 st = cudec_snappy_decompress_batch(d_src + j, d_sizes + j, d_dst + j, d_caps + j,
                                                    k - j, d_res + j, cs);
+            else if (fmts[j] == CUDEC_FORMAT_GDEFLATE)
+                st = cudec_gdeflate_decompress_batch(d_src + j, d_sizes + j, d_dst + j,
+                                                     d_caps + j, k - j, d_res + j, cs);
             else if (fmts[j] == CUDEC_FORMAT_ZSTD)
                 st = cudec_zstd_decompress_batch(d_src + j, d_sizes + j, d_dst + j, d_caps + j,
                                                  k - j, d_res + j, sl.zstd_ws.p, sl.zstd_ws.cap,

@@ -261,7 +261,8 @@ def mixed_batch(n, seed, formats=("lz4", "snappy"), median=16384, sigma=1.2, lo=
                 hi=4 << 20, random_frac=0.05, threads=None, weights=None, zstd_level=3):
     """The uneven mixed batch: lognormal sizes, copy probability uniform in
     0.2-0.8 per chunk, `random_frac` of the chunks uniform random bytes, the
-    format of chunk i = formats[i % len(formats)], or drawn with `weights`.
+    format of chunk i = formats[i % len(formats)], or drawn with `weights`;
+    a GDeflate chunk is one page, so its size is capped at 64 KiB.
     Returns (raws, comps, fmts) with raws as numpy views of one buffer."""
     sizes = mixed_sizes(n, seed, median, sigma, lo, hi)
     rng = np.random.default_rng(seed + 1)
@@ -272,7 +273,11 @@ def mixed_batch(n, seed, formats=("lz4", "snappy"), median=16384, sigma=1.2, lo=
     else:
         w = np.asarray(weights, dtype=np.float64)
         fmts = [formats[k] for k in rng.choice(len(formats), size=n, p=w / w.sum())]
-    params = [(zstd_params(float(p), 0.1) if f == "zstd" else lz_params(float(p), bool(r)))
+    # a GDeflate chunk is one page: at most 64 KiB
+    sizes = np.array([min(int(s), 65536) if f == "gdeflate" else int(s)
+                      for s, f in zip(sizes, fmts)], dtype=np.int64)
+    params = [(zstd_params(float(p), 0.1) if f == "zstd" else
+               gdeflate_params(float(p)) if f == "gdeflate" else lz_params(float(p), bool(r)))
               for p, r, f in zip(probs, rand, fmts)]
     for i, f in enumerate(fmts):
         if f == "zstd" and rand[i]:
@@ -286,6 +291,8 @@ def mixed_batch(n, seed, formats=("lz4", "snappy"), median=16384, sigma=1.2, lo=
             return lz4_compress(r)
         if f == "snappy":
             return snappy_compress(r)
+        if f == "gdeflate":
+            return gdeflate_compress(r.tobytes(), 6)
         return zstd_compress(r.tobytes(), zstd_level, 20, True)
 
     if n >= 256:

@@ -158,9 +158,40 @@ cudec_status cudec_zstd_decompress_batch_noalloc(const void* const* d_src_ptrs,
                                                  cudec_stream_t stream);
 
 /* ---------------------------------------------------------------------
+ * GDeflate (no decoder in the reference; its 32-lane refill schedule and
+ * TileStream envelope are src/gdeflate_schedule.h and src/tilestream.h). One
+ * page per chunk, at most 64 KiB out; the page format's open points are
+ * decided as documented with the decoder. Statuses: OUTPUT_TOO_SMALL when a
+ * page produces more than the capacity, CORRUPT_INPUT for every malformed
+ * page (including one that would produce more than 64 KiB or does not end
+ * exactly at its last word). */
+cudec_status cudec_gdeflate_decompress_batch(const void* const* d_src_ptrs,
+                                             const size_t* d_src_sizes,
+                                             void* const* d_dst_ptrs,
+                                             const size_t* d_dst_capacities,
+                                             size_t chunk_count,
+                                             cudec_chunk_result* d_results,
+                                             cudec_stream_t stream);
+
+/* One validated tile of a TileStream container. */
+typedef struct cudec_tile {
+    uint64_t src_offset; /* from the start of the stream */
+    uint64_t src_size;
+    uint64_t dst_size;
+} cudec_tile;
+
+/* The TileStream envelope walker (src/tilestream.h:117-261): host memory,
+ * no device work. INVALID_ARGUMENT for NULL arguments or a tile array smaller
+ * than the declared count; CORRUPT_INPUT for everything the bytes get wrong. */
+cudec_status cudec_gdeflate_tilestream_parse(const void* h_stream, size_t stream_size,
+                                             cudec_tile* tiles, size_t tiles_capacity,
+                                             size_t* out_tile_count, size_t* out_total);
+
+/* ---------------------------------------------------------------------
  * Mixed-format persistent batch decode (no counterpart in the reference; the
  * design record's batching direction). One launch decodes LZ4 blocks, raw
- * Snappy blocks and Zstd frames in any mix, with per-chunk statuses and bytes
+ * Snappy blocks, Zstd frames and GDeflate pages in any mix, with per-chunk
+ * statuses and bytes
  * identical to the per-format entries. A plan (bound to the device current at
  * creation) owns the device workspace (work counter, a largest-first chunk
  * order, Zstd literal slots), the decode shape per size bucket and a CUDA
@@ -274,6 +305,15 @@ typedef enum cudec_mem_space {
     CUDEC_MEM_HOST = 0,   /* host destinations; output is copied back */
     CUDEC_MEM_DEVICE = 1  /* device destinations; output stays in HBM */
 } cudec_mem_space;
+
+/* GDeflate TileStream container, synchronous: parse, one page-batch launch
+ * over every tile; each tile must produce exactly its size (else
+ * CORRUPT_INPUT; the first failing tile's status otherwise). dst is host or
+ * device memory per dst_space. */
+cudec_status cudec_gdeflate_tilestream_decompress(const void* h_stream, size_t stream_size,
+                                                  void* dst, size_t dst_capacity,
+                                                  cudec_mem_space dst_space,
+                                                  size_t* out_written);
 
 /* ---------------------------------------------------------------------
  * Streaming batch LZ4 block decode from HOST-resident chunks.

@@ -12,7 +12,7 @@
  * golden vectors anywhere in the reference: it follows the format description
  * the reference records (docs/MASTERPLAN.md:861-960, draft sections 5-11,
  * divergences D1-D6 from RFC 1951) plus the decisions listed at
- * `gd_decode_page`. Symbol-level parity with the GDeflate reference decoder is
+ * `oracle_gdeflate_decode`. Symbol-level parity with the GDeflate reference decoder is
  * therefore UNPINNED.
  */
 #include <stdint.h>
@@ -140,6 +140,7 @@ int oracle_gdeflate_schedule_trace(const uint8_t* page, uint64_t bytes, const ui
  * Canonical Huffman codes, read most-significant code bit first from the
  * lane's least-significant end (RFC 1951 section 3.1.1 bit order). */
 #define G_MAXBITS 15
+#define G_PAGE_MAX 65536u /* a page never produces more */
 
 typedef struct {
     uint16_t count[G_MAXBITS + 1];
@@ -226,9 +227,10 @@ static void round_rest(gsched* s) {
  *     end-of-block has been read and no distance is pending; symbols 286/287
  *     are CORRUPT;
  *   - stored blocks: LEN bytes as 8-bit atoms, byte 32r+l on lane l of round r;
- *   - checks per operation in this order: symbol, extra bits, output room
- *     (OUTPUT_TOO_SMALL), distance within the page output (CORRUPT); a
- *     refill with no word left is CORRUPT at that lane's refill turn;
+ *   - checks per operation in this order: symbol, extra bits, the page's
+ *     64 KiB output limit (CORRUPT), output room (OUTPUT_TOO_SMALL),
+ *     distance within the page output (CORRUPT); a refill with no word left
+ *     is CORRUPT at that lane's refill turn;
  *   - the page must be consumed exactly: after the final block's last round
  *     the schedule's word cursor must equal the page's word count.
  * cap is the output capacity (bytes_written <= cap). */
@@ -255,6 +257,7 @@ int oracle_gdeflate_decode(const uint8_t* page, uint64_t size, uint8_t* out, uin
                 for (uint32_t l = 0; l < G_LANES; ++l) {
                     if (r * 32u + l < len) {
                         const uint32_t b = gs_pop(&s, 8);
+                        if (pos >= G_PAGE_MAX) return G_CORRUPT;
                         if (pos >= cap) return G_TOO_SMALL;
                         out[pos++] = (uint8_t)b;
                     }
@@ -343,12 +346,14 @@ int oracle_gdeflate_decode(const uint8_t* page, uint64_t size, uint8_t* out, uin
                     const int sym = gh_decode(&s, &lit);
                     if (sym < 0 || sym > 285) return G_CORRUPT;
                     if (sym < 256) {
+                        if (pos >= G_PAGE_MAX) return G_CORRUPT;
                         if (pos >= cap) return G_TOO_SMALL;
                         out[pos++] = (uint8_t)sym;
                     } else if (sym == 256) {
                         eob_now = 1;
                     } else {
                         const uint64_t L = kLBase[sym - 257] + gs_pop(&s, kLExtra[sym - 257]);
+                        if (L > G_PAGE_MAX - pos) return G_CORRUPT;
                         if (L > cap - pos) return G_TOO_SMALL;
                         pend_pos[l] = pos;
                         pend_len[l] = L;

@@ -126,3 +126,22 @@ def test_page_mutants_are_refused_or_decoded_deterministically():
         assert a == oracle.gdeflate_decode(bytes(b), cap)
         statuses.add(a[0])
     assert statuses <= {0, 2, 3} and 2 in statuses
+
+
+def test_library_tilestream_walker_matches_reference_seeds():
+    """The shipped walker (cudec_gdeflate_tilestream_parse, host-only) gives
+    the reference walker's verdicts and tables on its fuzz seeds."""
+    import cudec_b200 as cd
+    vecs = json.load(open(os.path.join(GOLDEN, "tilestream.json")))["vectors"]
+    for v in vecs:
+        st, tiles, total = cd.tilestream_parse(bytes.fromhex(v["input_hex"]), v["tiles_capacity"])
+        assert st == v["expect_status"], v["name"]
+        if st == 0:
+            assert tiles == v["expect_tiles"] and total == v["expect_total"], v["name"]
+    rng = random.Random(29)
+    base = W.gdeflate_tilestream(bytes(rng.randrange(256) for _ in range(200000)), 1)
+    for _ in range(300):
+        b = bytearray(base[:64])
+        b[rng.randrange(40)] ^= 1 << rng.randrange(8)
+        cap = rng.choice([0, 1, 3, 4, 8])
+        assert cd.tilestream_parse(bytes(b), cap) == oracle.tilestream_parse(bytes(b), cap)

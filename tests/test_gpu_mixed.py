@@ -12,7 +12,9 @@ import cudec_b200 as cd
 import oracle
 from cudec_b200 import workload as W
 
-ORACLE = {"lz4": oracle.lz4_decode, "snappy": oracle.snappy_decode, "zstd": oracle.zstd_decode}
+ORACLE = {"lz4": oracle.lz4_decode, "snappy": oracle.snappy_decode, "zstd": oracle.zstd_decode,
+          "gdeflate": oracle.gdeflate_decode}
+FORMATS = ("lz4", "snappy", "zstd", "gdeflate")
 
 pytestmark = pytest.mark.gpu
 
@@ -25,7 +27,7 @@ def mutate(b, rng):
 
 
 def make_batch(n, seed, hi=1 << 20):
-    raws, comps, fmts = W.mixed_batch(n, seed, formats=("lz4", "snappy", "zstd"), hi=hi)
+    raws, comps, fmts = W.mixed_batch(n, seed, formats=FORMATS, hi=hi)
     rng = random.Random(seed)
     comps = [bytes(c) for c in comps]
     caps = [len(r) for r in raws]
@@ -45,7 +47,7 @@ def per_format(cuda, comps, caps, fmts):
     import torch
     from cudec_b200.device import DeviceBatch
     recs, outs = [None] * len(comps), [None] * len(comps)
-    for f in ("lz4", "snappy", "zstd"):
+    for f in FORMATS:
         idx = [i for i, x in enumerate(fmts) if x == f]
         if not idx:
             continue
@@ -105,7 +107,7 @@ def test_new_arguments_recapture_and_unknown_codes(cuda):
         recs, outs = per_format(cuda, comps, caps, fmts)
         codes = [cd.FORMAT_CODES[f] for f in fmts]
         codes[3] = 9
-        codes[7] = cd.FORMAT_GDEFLATE
+        codes[7] = 200
         recs[3] = recs[7] = (cd.ERR_UNSUPPORTED, 0)
         b = DeviceBatch(comps, caps, device=cuda)
         assert b.run_mixed(plan, codes) == 0

@@ -16,7 +16,8 @@ from cudec_b200.device import read_device
 
 pytestmark = pytest.mark.gpu
 
-ORACLE = {"lz4": oracle.lz4_decode, "snappy": oracle.snappy_decode, "zstd": oracle.zstd_decode}
+ORACLE = {"lz4": oracle.lz4_decode, "snappy": oracle.snappy_decode, "zstd": oracle.zstd_decode,
+          "gdeflate": oracle.gdeflate_decode}
 
 
 def make_requests(k, seed, max_n=300, hi=256 << 10):
@@ -24,7 +25,8 @@ def make_requests(k, seed, max_n=300, hi=256 << 10):
     reqs = []
     for i in range(k):
         n = int(round(np.exp(rng.uniform(0, np.log(max_n)))))
-        raws, comps, fmts = W.mixed_batch(n, seed * 1000 + i, formats=("lz4", "snappy", "zstd"),
+        raws, comps, fmts = W.mixed_batch(n, seed * 1000 + i,
+                                          formats=("lz4", "snappy", "zstd", "gdeflate"),
                                           median=32768, sigma=1.0, lo=512, hi=hi)
         caps = [len(r) for r in raws]
         if n > 3:
