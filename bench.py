@@ -28,6 +28,12 @@ the launch itself is bracketed by CUDA events on its stream.
             uniform 0.2-0.8 per chunk, 5 % incompressible chunks, half LZ4 and
             half Snappy; the persistent work-stealing plan (tuned once, CUDA
             graph) against the plain path (one batch launch per format)
+  gdeflate  4 GiB as 65,536 pages of 64 KiB in 16,384 TileStreams of
+            256 KiB (content: 256-symbol Zipf(1.3) literals, matches 3-258,
+            offsets up to 32 KiB), encoded by this build's GDeflate encoder at
+            its highest effort (dynamic Huffman blocks); `--gdeflate-unique`
+            distinct streams are encoded and laid out repeatedly, every page
+            its own copy in HBM; one page-batch launch
   serve     the served mixed-format stream: Poisson arrivals, each request
             1-4,096 chunks (log-uniform), 40 % LZ4 / 20 % Snappy / 30 % Zstd
             level 3 (the 10 % GDeflate share is left out until that decoder
@@ -84,6 +90,10 @@ def parse_args():
                     help="requests of the served mixed-format stream (0 skips it)")
     ap.add_argument("--serve-rate", type=float, default=200.0,
                     help="Poisson arrival rate of the served stream (requests/s)")
+    ap.add_argument("--gdeflate-streams", type=int, default=16384,
+                    help="256 KiB TileStreams of the GDeflate leg (0 skips it)")
+    ap.add_argument("--gdeflate-unique", type=int, default=512,
+                    help="distinct TileStreams encoded for the GDeflate leg")
     ap.add_argument("--zstd-frames", type=int, default=4096,
                     help="Zstd frames per batch (0 skips the Zstd legs)")
     ap.add_argument("--zstd-unique", type=int, default=128,
@@ -329,6 +339,54 @@ def run_mixed(torch, cd, DeviceBatch, args, dev, stream, flush, max_over_ranks, 
     }
 
 
+GD_SEED = 0xC0DEC3
+
+
+def _gd_job(i):
+    from cudec_b200 import workload as W
+    sizes = [65536] * 4
+    buf, _ = W.generate(sizes, [W.gdeflate_params(0.5)],
+                        seeds=np.array([W.chunk_seed(GD_SEED, 3, 4 * i + k) for k in range(4)],
+                                       dtype=np.uint64))
+    raw = buf.tobytes()
+    return raw, W.gdeflate_tilestream(raw, 12, 32768)
+
+
+def run_gdeflate(torch, cd, DeviceBatch, args, dev, stream, flush, max_over_ranks, world, warm):
+    """65,536 GDeflate pages (16,384 TileStreams x 4 tiles) in one launch."""
+    import multiprocessing as mp
+    unique = min(args.gdeflate_unique, args.gdeflate_streams)
+    with mp.get_context("spawn").Pool(min(os.cpu_count() or 1, 32)) as pool:
+        made = pool.map(_gd_job, range(unique))
+    pages, raws = [], []
+    for raw, ts in made:
+        st, tiles, total = cd.tilestream_parse(ts, 4)
+        assert st == 0 and total == len(raw)
+        for k, (off, sz, dsz) in enumerate(tiles):
+            pages.append(ts[off:off + sz])
+            raws.append(raw[65536 * k:65536 * k + dsz])
+    n = 4 * args.gdeflate_streams
+    comps = [pages[i % len(pages)] for i in range(n)]
+    b = DeviceBatch(comps, [65536] * n, device=dev, poison=None)
+    ms = max_over_ranks(time_device(torch, b, "gdeflate", stream, flush,
+                                    max(args.steps // 50, 3), warm))
+    res = b.results()
+    assert (res["status"] == 0).all() and (res["bytes_written"] == 65536).all()
+    for i in range(0, n, max(n // 32, 1)):
+        o = int(b.dst_offs[i])
+        assert b.d_dst[o:o + 65536].cpu().numpy().tobytes() == raws[i % len(raws)]
+    out_bytes = 65536 * n
+    in_bytes = b.src_bytes
+    del b
+    torch.cuda.empty_cache()
+    return {"value": round(world * out_bytes / (ms * 1e-3) / 1e9, 3), "ms_per_step": round(ms, 3),
+            "pages": n, "streams": args.gdeflate_streams, "unique_streams": unique,
+            "compressed_bytes": in_bytes, "decompressed_bytes": out_bytes,
+            "roofline_frac": round((in_bytes + out_bytes) / (ms * 1e-3) / 1e9 / peaks()[0], 5),
+            "encoder": "this build's GDeflate encoder, level 12, 32 KiB window",
+            "parity": "vs the build's CPU decoder; GDeflate reference decoder unpinned"}
+
+
 SERVE_SEED = 0xC0DEC5
 SERVE_SLOTS = 32
 
@@ -508,6 +566,12 @@ def main():
         mixed_line = run_mixed(torch, cd, DeviceBatch, args, dev, stream, flush,
                                max_over_ranks, world, warm)
 
+    # ---- GDeflate pages (TileStream tiles) ------------------------------
+    gd_line = None
+    if args.gdeflate_streams > 0:
+        gd_line = run_gdeflate(torch, cd, DeviceBatch, args, dev, stream, flush,
+                               max_over_ranks, world, warm)
+
     # ---- served stream: continuous batching vs the plain queue --------
     serve_line = None
     if args.serve_requests > 0:
@@ -603,6 +667,7 @@ def main():
                            "ms_per_step": round(s_ms, 5),
                            "roofline_frac": round((s_in + out_bytes) / (s_ms * 1e-3) / 1e9 / peak, 5)},
                 **zstd_lines,
+                **({"gdeflate": gd_line} if gd_line else {}),
             },
             **({"mixed": mixed_line} if mixed_line else {}),
             **({"serve": serve_line} if serve_line else {}),

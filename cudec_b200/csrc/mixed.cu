@@ -113,6 +113,31 @@ __global__ void order_place(const size_t* caps, size_t n, Ctrl* ctrl, uint32_t* 
     }
 }
 
+// Each format's path is an out-of-line call, compiled as in its own kernel:
+// one decoder's register demand does not shape another's allocation.
+template <class F>
+__device__ __noinline__ int mixed_lz(const uint8_t* src, uint64_t S, uint8_t* dst, uint64_t cap,
+                                     uint8_t* base, lzw::Tune tn, uint32_t lane,
+                                     uint64_t* written) {
+    return lzw::decode_chunk<F>(src, S, dst, cap, base, base + lzw::kRing,
+                                reinterpret_cast<uint16_t*>(base + lzw::kRing + lzw::kIn), tn,
+                                lane, written);
+}
+
+__device__ __noinline__ int mixed_zstd(const uint8_t* src, uint64_t S, uint8_t* dst, uint64_t cap,
+                                       uint8_t* base, uint8_t* litbuf, uint32_t lane,
+                                       uint64_t* written) {
+    return zstd::decode_frame(src, S, dst, cap, *reinterpret_cast<zstd::WarpSmem*>(base), litbuf,
+                              lane, written);
+}
+
+__device__ __noinline__ int mixed_gdeflate(const uint8_t* src, uint64_t S, uint8_t* dst,
+                                           uint64_t cap, uint8_t* base, uint32_t lane,
+                                           uint64_t* written) {
+    return gdf::decode_page<false>(src, S, dst, cap, nullptr, *reinterpret_cast<gdf::Tables*>(base),
+                                   lane, written);
+}
+
 __global__ void __launch_bounds__(kThreads) mixed_kernel(Args a) {
     extern __shared__ __align__(16) uint8_t mixed_smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -132,25 +157,18 @@ __global__ void __launch_bounds__(kThreads) mixed_kernel(Args a) {
         int st;
         switch (a.formats[c]) {
             case CUDEC_FORMAT_LZ4:
-                st = lzw::decode_chunk<lzw::Lz4>(
-                    src, S, dst, cap, base, base + lzw::kRing,
-                    reinterpret_cast<uint16_t*>(base + lzw::kRing + lzw::kIn),
-                    a.tune[size_bucket(cap)], lane, &written);
+                st = mixed_lz<lzw::Lz4>(src, S, dst, cap, base, a.tune[size_bucket(cap)], lane,
+                                        &written);
                 break;
             case CUDEC_FORMAT_SNAPPY:
-                st = lzw::decode_chunk<lzw::Snappy>(
-                    src, S, dst, cap, base, base + lzw::kRing,
-                    reinterpret_cast<uint16_t*>(base + lzw::kRing + lzw::kIn),
-                    a.tune[size_bucket(cap)], lane, &written);
+                st = mixed_lz<lzw::Snappy>(src, S, dst, cap, base, a.tune[size_bucket(cap)], lane,
+                                           &written);
                 break;
             case CUDEC_FORMAT_GDEFLATE:
-                st = gdf::decode_page<false>(src, S, dst, cap, nullptr,
-                                             *reinterpret_cast<gdf::Tables*>(base), lane,
-                                             &written);
+                st = mixed_gdeflate(src, S, dst, cap, base, lane, &written);
                 break;
             case CUDEC_FORMAT_ZSTD:
-                st = zstd::decode_frame(src, S, dst, cap, *reinterpret_cast<zstd::WarpSmem*>(base),
-                                        litbuf, lane, &written);
+                st = mixed_zstd(src, S, dst, cap, base, litbuf, lane, &written);
                 break;
             default:
                 st = CUDEC_ERR_UNSUPPORTED;
