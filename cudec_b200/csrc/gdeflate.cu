@@ -16,19 +16,21 @@
 namespace cdb {
 namespace gdf {
 
-constexpr int kSmem = static_cast<int>(sizeof(Smem));
+constexpr uint32_t kWarps = 4;
+constexpr int kSmem = static_cast<int>(kWarps * sizeof(Tables));
 
-__global__ void __launch_bounds__(32)
+__global__ void __launch_bounds__(32 * kWarps)
     gdeflate_kernel(const void* const* src_ptrs, const size_t* src_sizes, void* const* dst_ptrs,
                     const size_t* dst_caps, size_t n, cudec_chunk_result* results) {
     extern __shared__ __align__(16) uint8_t gdf_smem[];
-    Smem& sm = *reinterpret_cast<Smem*>(gdf_smem);
-    const uint32_t lane = threadIdx.x & 31;
-    for (size_t c = blockIdx.x; c < n; c += gridDim.x) {
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    Tables& tb = reinterpret_cast<Tables*>(gdf_smem)[warp];
+    const size_t total = static_cast<size_t>(gridDim.x) * kWarps;
+    for (size_t c = static_cast<size_t>(blockIdx.x) * kWarps + warp; c < n; c += total) {
         uint64_t written = 0;
-        const int st = decode_page<true>(static_cast<const uint8_t*>(src_ptrs[c]), src_sizes[c],
-                                         static_cast<uint8_t*>(dst_ptrs[c]), dst_caps[c], sm.out,
-                                         sm.t, lane, &written);
+        const int st = decode_page(static_cast<const uint8_t*>(src_ptrs[c]), src_sizes[c],
+                                   static_cast<uint8_t*>(dst_ptrs[c]), dst_caps[c], tb, lane,
+                                   &written);
         __syncwarp();
         if (lane == 0) {
             results[c].status = st;
@@ -51,7 +53,7 @@ cudaError_t prepare(int dev, int* per_sm) {
     cudaError_t e = cudaFuncSetAttribute(gdeflate_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, gdeflate_kernel, 32, kSmem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, gdeflate_kernel, 32 * kWarps, kSmem);
     if (e != cudaSuccess) return e;
     if (v <= 0) return cudaErrorInvalidConfiguration;
     g_ready[dev].store(v, std::memory_order_release);
@@ -123,8 +125,9 @@ cudec_status cudec_gdeflate_decompress_batch(const void* const* d_src_ptrs,
     const int sms = cdb::device_sm_count(dev);
     if (sms <= 0) return CUDEC_ERR_CUDA;
     const size_t max_blocks = static_cast<size_t>(sms) * per_sm;
-    const unsigned grid = static_cast<unsigned>(chunk_count < max_blocks ? chunk_count : max_blocks);
-    cdb::gdf::gdeflate_kernel<<<grid, 32, cdb::gdf::kSmem,
+    const size_t want = (chunk_count + cdb::gdf::kWarps - 1) / cdb::gdf::kWarps;
+    const unsigned grid = static_cast<unsigned>(want < max_blocks ? want : max_blocks);
+    cdb::gdf::gdeflate_kernel<<<grid, 32 * cdb::gdf::kWarps, cdb::gdf::kSmem,
                                 reinterpret_cast<cudaStream_t>(stream)>>>(
         d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_capacities, chunk_count, d_results);
     return cudaGetLastError() == cudaSuccess ? CUDEC_OK : CUDEC_ERR_CUDA;

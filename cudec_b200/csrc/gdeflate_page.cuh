@@ -15,9 +15,11 @@
 // memory, canonical decoding for longer codes; the precode has a complete
 // 7-bit table. End-of-block quiesce is a ballot: lanes after the first lane
 // that read end-of-block (and have no distance pending) do not consume.
-// Output positions come from a warp scan of the round's item lengths. The
-// whole page output (at most 64 KiB) is assembled in shared memory, so
-// copies never read global memory; it leaves with aligned vector stores.
+// Output positions come from a warp scan of the round's item lengths; bytes
+// go straight to the destination (a page is at most 64 KiB) and copies read
+// them back from there. Shared memory holds only the tables (about 6 KB per
+// warp), so many pages decode per SM: staging the page in shared memory
+// measured 5x slower for lack of resident warps.
 //
 // Errors are reported in serial order: an operation's error at lane l
 // precedes lane l's refill, which precedes lane l+1's operation.
@@ -26,7 +28,6 @@
 #include <cstdint>
 
 #include "cudec.h"
-#include "lz_warp_kernel.cuh"
 
 namespace cdb {
 namespace gdf {
@@ -47,11 +48,6 @@ struct __align__(16) Tables {
     uint8_t plen[20];
 };
 
-// Tables plus the page assembled in shared memory (the staged decode).
-struct __align__(16) Smem {
-    uint8_t out[kPageMax];
-    Tables t;
-};
 
 static __constant__ uint16_t kLBase[29] = {3,  4,  5,  6,  7,  8,  9,  10,  11,  13,
                                     15, 17, 19, 23, 27, 31, 35, 43,  51,  59,
@@ -212,16 +208,15 @@ __device__ __forceinline__ void page_copy(uint8_t* out, uint32_t o, uint32_t n, 
     for (uint32_t k = 0; k < n; ++k) out[o + k] = out[o - d + k];
 }
 
-// Decode one page; every lane returns the same status and *written. With
-// kStaged the page is assembled in `page` (shared memory, 64 KiB) and leaves
-// at the end with aligned vector stores; otherwise it is written straight to
-// dst and copies read it back from there.
-template <bool kStaged>
+// Decode one page; every lane returns the same status and *written. Output
+// goes straight to dst (its bytes are only ever read back by this warp's own
+// copies, ordered by __syncwarp), so a warp needs only its tables in shared
+// memory and many warps share an SM.
 __device__ __forceinline__ int decode_page(const uint8_t* pg, uint64_t N, uint8_t* dst,
-                                           uint64_t cap, uint8_t* page, Tables& sm,
-                                           uint32_t lane, uint64_t* written) {
+                                           uint64_t cap, Tables& sm, uint32_t lane,
+                                           uint64_t* written) {
     *written = 0;
-    uint8_t* const out = kStaged ? page : dst;
+    uint8_t* const out = dst;
     if (N % 4 != 0 || N / 4 < 32) return CUDEC_ERR_CORRUPT_INPUT;
     Lane ln{pg, (reinterpret_cast<uintptr_t>(pg) & 3) == 0, N / 4, 32, 0, 32};
     ln.bb = ln.word(lane);
@@ -433,23 +428,6 @@ __device__ __forceinline__ int decode_page(const uint8_t* pg, uint64_t N, uint8_
     }
     if (ln.cursor != ln.words) return CUDEC_ERR_CORRUPT_INPUT;
     __syncwarp();
-    if (!kStaged) {
-        *written = pos;
-        return CUDEC_OK;
-    }
-    // ---- page out: aligned 16-byte stores ----
-    const uintptr_t da = reinterpret_cast<uintptr_t>(dst);
-    uint32_t head = static_cast<uint32_t>((16 - (da & 15)) & 15);
-    if (head > pos) head = pos;
-    if (lane < head) dst[lane] = page[lane];
-    const uint32_t body_end = head + ((pos - head) & ~15u);
-    for (uint32_t k = head + 16 * lane; k < body_end; k += 512) {
-        const uint32_t mis = k & 15;
-        const uint4 lo = *reinterpret_cast<const uint4*>(page + (k - mis));
-        const uint4 hi = *reinterpret_cast<const uint4*>(page + (k - mis) + 16);
-        *reinterpret_cast<uint4*>(dst + k) = lzw::shift32(lo, hi, mis);
-    }
-    if (body_end + lane < pos) dst[body_end + lane] = page[body_end + lane];
     *written = pos;
     return CUDEC_OK;
 }

@@ -2,8 +2,7 @@
 //
 // One launch decodes a batch whose chunks are LZ4 blocks, raw Snappy blocks,
 // Zstd frames and GDeflate pages in any mix and of any sizes (a per-chunk
-// format code; GDeflate pages are written straight to their destinations
-// here, the tables in the warp's shared memory). A
+// format code). A
 // plan owns everything the launch needs so the call allocates nothing:
 //
 //   * a largest-first order of the chunks (by output capacity), built on the
@@ -134,8 +133,8 @@ __device__ __noinline__ int mixed_zstd(const uint8_t* src, uint64_t S, uint8_t* 
 __device__ __noinline__ int mixed_gdeflate(const uint8_t* src, uint64_t S, uint8_t* dst,
                                            uint64_t cap, uint8_t* base, uint32_t lane,
                                            uint64_t* written) {
-    return gdf::decode_page<false>(src, S, dst, cap, nullptr, *reinterpret_cast<gdf::Tables*>(base),
-                                   lane, written);
+    return gdf::decode_page(src, S, dst, cap, *reinterpret_cast<gdf::Tables*>(base), lane,
+                            written);
 }
 
 __global__ void __launch_bounds__(kThreads) mixed_kernel(Args a) {
