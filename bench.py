@@ -505,11 +505,10 @@ def main():
     import cudec_b200 as cd
     from cudec_b200.device import DeviceBatch
 
+    from cudec_b200 import replicas
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    replicas.init("nccl", dev)
     cd.lib()
     n = args.chunks
     warm = max(args.warmup, 3)
@@ -537,11 +536,7 @@ def main():
         torch.cuda.synchronize(dev)
 
     def max_over_ranks(x):
-        if world > 1:
-            t = torch.tensor([x], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return x
+        return replicas.max_over_ranks(x, dev)
 
     barrier()
     with ClockSampler(local) as clocks:
@@ -689,8 +684,7 @@ def main():
                                  "library": "liblz4 %d LZ4_decompress_safe"
                                             % oracle.oracle_lib().codec_lz4_version()}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finish()
 
 
 if __name__ == "__main__":

@@ -755,13 +755,69 @@ __device__ __forceinline__ void exec_small(Out& out, const In& in, bool act, uin
     out.flush(bend, false, lane);
 }
 
-// Decode one chunk with the calling warp. Returns the status; *written is
-// the output length on success.
-template <class F>
-__device__ __forceinline__ int decode_chunk(const uint8_t* g, uint64_t S, uint8_t* dst, uint64_t cap,
-                            uint8_t* ring, uint8_t* win, uint16_t* tab, const Tune& tn,
-                            uint32_t lane, uint64_t* written) {
-    *written = 0;
+// One token of a group as a lane holds it: literal run li bytes from input
+// position lsrc to output position o, then a match of mi bytes at offset off.
+struct Tok {
+    uint64_t o, li, lsrc, mi;
+    uint32_t off;
+};
+
+// Executes checked groups of tokens: tokens of at most kBig bytes lane-
+// parallel through the output ring (batches of up to tn.batch bytes), longer
+// ones by the whole warp straight to the destination. Literal bytes come
+// from the input window when `in` holds them, else from global memory.
+struct ExecSink {
+    Out out;
+    const uint8_t* g;
+    uint8_t* dst;
+    const In* in;
+    Tune tn;
+    uint32_t lane;
+
+    __device__ __forceinline__ void group(const Tok& t, uint32_t m) {
+        const bool act = lane < m;
+        const uint64_t tend = t.o + t.li + t.mi;
+        const bool big = act && t.li + t.mi > kBig;
+        uint32_t s0 = 0;
+        while (s0 < m) {
+            const uint64_t os = __shfl_sync(kFull, t.o, s0);
+            const unsigned cut =
+                __ballot_sync(kFull, act && lane >= s0 && (big || tend - os > tn.batch));
+            const uint32_t e = cut ? __ffs(cut) - 1 : m;
+            if (e == s0) {
+                const uint64_t bo = os;
+                const uint64_t bli = __shfl_sync(kFull, t.li, s0);
+                const uint64_t bls = __shfl_sync(kFull, t.lsrc, s0);
+                const uint64_t bmi = __shfl_sync(kFull, t.mi, s0);
+                const uint32_t boff = __shfl_sync(kFull, t.off, s0);
+                out.flush(bo, true, lane);
+                if (bli) coop_literal(dst, bo, g + bls, bli, lane);
+                __syncwarp();
+                if (bmi) coop_match(dst, bo + bli, bmi, boff, out.ring, lane);
+                __syncwarp();
+                out.flushed = out.vlo = bo + bli + bmi;
+                LZW_EV(3, 1);
+                ++s0;
+                continue;
+            }
+            const uint64_t bend = __shfl_sync(kFull, tend, e - 1);
+            exec_small(out, *in, act && lane >= s0 && lane < e, t.o, t.li, t.lsrc, t.mi, t.off,
+                       bend, lane);
+            s0 = e;
+        }
+    }
+    __device__ __forceinline__ void finish(uint64_t d) { out.flush(d, true, lane); }
+};
+
+// Parses one chunk (window tables, hop composition, the exact ladder per
+// token) and hands every checked group of up to 32 tokens to the sink in
+// chain order: sink.group(tok, m, last, dend) returns false to abandon the
+// chunk. Returns the chunk's status; *dend is the output length on success.
+template <class F, class Sink>
+__device__ __forceinline__ int parse_chunk(const uint8_t* g, uint64_t S, uint64_t cap,
+                                           uint8_t* win, uint16_t* tab, const Tune& tn,
+                                           uint32_t lane, Sink& sink, In& in, uint64_t* dend_out) {
+    *dend_out = 0;
     uint64_t p, limit;
     int status = F::begin(g, S, cap, &p, &limit);
     if (status != CUDEC_OK) return status;
@@ -769,10 +825,9 @@ __device__ __forceinline__ int decode_chunk(const uint8_t* g, uint64_t S, uint8_
     const uintptr_t gbase = reinterpret_cast<uintptr_t>(g);
     Filler fill{g, win, gbase, S, -static_cast<int64_t>(gbase & 15),
                 -static_cast<int64_t>(gbase & 15)};
-    In in{g, win, gbase, 0, 0};
+    in = In{g, win, gbase, 0, 0};
     fill.issue(p, p + tn.ahead, lane);
-    Out out{ring, dst, reinterpret_cast<uintptr_t>(dst), 0, 0};
-    uint64_t d = 0;  // output position of the next token; all before it executed
+    uint64_t d = 0;  // output position of the next token
     LZW_T(t_chunk);
     for (;;) {
         LZW_T(t_land);
@@ -787,6 +842,7 @@ __device__ __forceinline__ int decode_chunk(const uint8_t* g, uint64_t S, uint8_
         LZW_ADD(0, t_land);
         if (F::at_end(p, S)) {
             status = F::finish(d, limit);
+            if (status == CUDEC_OK && !sink.group(Tok{}, 0, true, d)) status = CUDEC_ERR_CUDA;
             break;
         }
         LZW_T(t_tab);
@@ -811,13 +867,13 @@ __device__ __forceinline__ int decode_chunk(const uint8_t* g, uint64_t S, uint8_
                 const int e = __ffs(ev) - 1;
                 const int se = __shfl_sync(kFull, st, e);
                 if (se != CUDEC_OK) {
-                    asm volatile("cp.async.wait_all;" ::: "memory");
-                    return se;
+                    status = se;
+                    last = true;
+                    break;
                 }
                 m = e + 1;
                 last = true;
             }
-            const bool act = lane < m;
             const uint64_t tend = dl + sq.lit + sq.ml;
             const uint64_t nxt = __shfl_sync(kFull, sq.next, m - 1);
             const uint64_t dend = __shfl_sync(kFull, tend, m - 1);
@@ -825,34 +881,10 @@ __device__ __forceinline__ int decode_chunk(const uint8_t* g, uint64_t S, uint8_
             LZW_EV(0, 1);
             LZW_EV(1, m);
             LZW_T(t_exec);
-            // ---- execute them in ring batches; long tokens by the warp ----
-            const bool big = act && sq.lit + sq.ml > kBig;
-            uint32_t s0 = 0;
-            while (s0 < m) {
-                const uint64_t os = __shfl_sync(kFull, dl, s0);
-                const unsigned cut =
-                    __ballot_sync(kFull, act && lane >= s0 && (big || tend - os > tn.batch));
-                const uint32_t e = cut ? __ffs(cut) - 1 : m;
-                if (e == s0) {
-                    const uint64_t bo = os;
-                    const uint64_t bli = __shfl_sync(kFull, sq.lit, s0);
-                    const uint64_t bls = __shfl_sync(kFull, sq.lit_src, s0);
-                    const uint64_t bmi = __shfl_sync(kFull, sq.ml, s0);
-                    const uint32_t boff = __shfl_sync(kFull, sq.off, s0);
-                    out.flush(bo, true, lane);
-                    if (bli) coop_literal(dst, bo, g + bls, bli, lane);
-                    __syncwarp();
-                    if (bmi) coop_match(dst, bo + bli, bmi, boff, ring, lane);
-                    __syncwarp();
-                    out.flushed = out.vlo = bo + bli + bmi;
-                    LZW_EV(3, 1);
-                    ++s0;
-                    continue;
-                }
-                const uint64_t bend = __shfl_sync(kFull, tend, e - 1);
-                exec_small(out, in, act && lane >= s0 && lane < e, dl, sq.lit, sq.lit_src,
-                           sq.ml, sq.off, bend, lane);
-                s0 = e;
+            if (!sink.group(Tok{dl, sq.lit, sq.lit_src, sq.ml, sq.off}, m, last, dend)) {
+                status = CUDEC_ERR_CUDA;
+                last = true;
+                break;
             }
             d = dend;
             LZW_ADD(3, t_exec);
@@ -866,13 +898,36 @@ __device__ __forceinline__ int decode_chunk(const uint8_t* g, uint64_t S, uint8_
         }
         if (last) break;
     }
-    if (status != CUDEC_OK) {
-        asm volatile("cp.async.wait_all;" ::: "memory");
-        return status;
-    }
     asm volatile("cp.async.wait_all;" ::: "memory");
-    out.flush(d, true, lane);
     LZW_ADD(5, t_chunk);
+    if (status != CUDEC_OK) return status;
+    *dend_out = d;
+    return CUDEC_OK;
+}
+
+// The single-warp sink: execute each group as soon as it is checked.
+struct DirectSink {
+    ExecSink* ex;
+    __device__ __forceinline__ bool group(const Tok& t, uint32_t m, bool, uint64_t) {
+        ex->group(t, m);
+        return true;
+    }
+};
+
+// Decode one chunk with the calling warp. Returns the status; *written is
+// the output length on success.
+template <class F>
+__device__ __forceinline__ int decode_chunk(const uint8_t* g, uint64_t S, uint8_t* dst, uint64_t cap,
+                            uint8_t* ring, uint8_t* win, uint16_t* tab, const Tune& tn,
+                            uint32_t lane, uint64_t* written) {
+    *written = 0;
+    In in{g, win, reinterpret_cast<uintptr_t>(g), 0, 0};
+    ExecSink ex{Out{ring, dst, reinterpret_cast<uintptr_t>(dst), 0, 0}, g, dst, &in, tn, lane};
+    DirectSink sink{&ex};
+    uint64_t d = 0;
+    const int st = parse_chunk<F>(g, S, cap, win, tab, tn, lane, sink, in, &d);
+    if (st != CUDEC_OK) return st;
+    ex.finish(d);
     *written = d;
     return CUDEC_OK;
 }

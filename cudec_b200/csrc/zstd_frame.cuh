@@ -7,10 +7,27 @@
 #include <cstdint>
 
 #include "cudec.h"
+#include "lz_warp_kernel.cuh"
 #include "zstd_kernel.cuh"
 
 namespace cdb {
 namespace zstd {
+
+// Profiling builds (-DCDB_PHASE_TIMING) accumulate per-phase SM cycles and
+// event counts over all frames of a launch.
+#ifdef CDB_PHASE_TIMING
+__device__ unsigned long long zs_cycles[8];
+__device__ unsigned long long zs_events[8];
+#define ZS_T(v) const long long v = clock64()
+#define ZS_ADD(i, t0) \
+    if (lane == 0) atomicAdd(&zs_cycles[i], static_cast<unsigned long long>(clock64() - (t0)))
+#define ZS_EV(i, n) \
+    if (lane == 0) atomicAdd(&zs_events[i], static_cast<unsigned long long>(n))
+#else
+#define ZS_T(v)
+#define ZS_ADD(i, t0)
+#define ZS_EV(i, n)
+#endif
 
 // XXH64 of p[0, n) with seed 0 (public xxHash specification), one lane.
 __device__ inline uint64_t xxh64_dev(const uint8_t* p, uint64_t n) {
@@ -67,13 +84,89 @@ __device__ __forceinline__ uint64_t warp_min64(uint64_t v) {
     return v;
 }
 
-// Warp-strided byte copy / fill (no overlap between src and dst ranges).
+// Copies and fills. Sources are read with ordinary (coherent) loads: literal
+// bytes in the workspace and match sources in the destination were written
+// by this warp earlier in the same launch. A 16-byte window of a source is
+// two aligned block loads and a funnel shift (lzw::ld16_output), never a load
+// of a block that holds no requested byte.
+
+constexpr uint64_t kLaneCopyMax = 64;  // longer runs are copied by the whole warp
+
+// The whole warp copies n bytes src -> dst (non-overlapping): destination-
+// aligned 16-byte stores, four in flight per lane.
 __device__ __forceinline__ void warp_copy(uint8_t* dst, const uint8_t* src, uint64_t n,
                                           uint32_t lane) {
-    for (uint64_t i = lane; i < n; i += 32) dst[i] = src[i];
+    uint64_t head = (16 - (reinterpret_cast<uintptr_t>(dst) & 15)) & 15;
+    if (head > n) head = n;
+    if (lane < head) dst[lane] = src[lane];
+    const uint64_t body_end = head + ((n - head) & ~15ull);
+    uint64_t k = head + 16ull * lane;
+    for (; k + 3 * 512 < body_end; k += 4 * 512) {
+        const uint4 v0 = lzw::ld16_output(src + k, 16), v1 = lzw::ld16_output(src + k + 512, 16);
+        const uint4 v2 = lzw::ld16_output(src + k + 1024, 16);
+        const uint4 v3 = lzw::ld16_output(src + k + 1536, 16);
+        *reinterpret_cast<uint4*>(dst + k) = v0;
+        *reinterpret_cast<uint4*>(dst + k + 512) = v1;
+        *reinterpret_cast<uint4*>(dst + k + 1024) = v2;
+        *reinterpret_cast<uint4*>(dst + k + 1536) = v3;
+    }
+    for (; k < body_end; k += 512) *reinterpret_cast<uint4*>(dst + k) = lzw::ld16_output(src + k, 16);
+    if (body_end + lane < n) dst[body_end + lane] = src[body_end + lane];
 }
+
+// The whole warp writes n copies of byte b.
 __device__ __forceinline__ void warp_fill(uint8_t* dst, uint8_t b, uint64_t n, uint32_t lane) {
-    for (uint64_t i = lane; i < n; i += 32) dst[i] = b;
+    uint64_t head = (16 - (reinterpret_cast<uintptr_t>(dst) & 15)) & 15;
+    if (head > n) head = n;
+    if (lane < head) dst[lane] = b;
+    const uint64_t body_end = head + ((n - head) & ~15ull);
+    const uint32_t w = 0x01010101u * b;
+    const uint4 v = make_uint4(w, w, w, w);
+    for (uint64_t k = head + 16ull * lane; k < body_end; k += 512)
+        *reinterpret_cast<uint4*>(dst + k) = v;
+    if (body_end + lane < n) dst[body_end + lane] = b;
+}
+
+// One lane copies n (<= kLaneCopyMax) bytes src -> dst, 16 at a time.
+__device__ __forceinline__ void lane_copy(uint8_t* dst, const uint8_t* src, uint64_t n) {
+    for (uint64_t k = 0; k < n; k += 16) {
+        const uint32_t m = n - k < 16 ? static_cast<uint32_t>(n - k) : 16u;
+        lzw::st16_global(dst + k, lzw::ld16_output(src + k, m), m);
+    }
+}
+
+__device__ __forceinline__ void lane_fill(uint8_t* dst, uint8_t b, uint64_t n) {
+    const uint32_t w = 0x01010101u * b;
+    const uint4 v = make_uint4(w, w, w, w);
+    for (uint64_t k = 0; k < n; k += 16)
+        lzw::st16_global(dst + k, v, n - k < 16 ? static_cast<uint32_t>(n - k) : 16u);
+}
+
+// One lane writes the match dst[ms, ms + n) at offset off (every byte before
+// ms is written): 16-byte steps, or for off < 16 the period replicated in
+// registers.
+__device__ __forceinline__ void lane_match(uint8_t* dst, uint64_t ms, uint64_t n, uint64_t off) {
+    uint8_t* o = dst + ms;
+    if (off >= 16) {
+        for (uint64_t k = 0; k < n; k += 16) {
+            const uint32_t m = n - k < 16 ? static_cast<uint32_t>(n - k) : 16u;
+            lzw::st16_global(o + k, lzw::ld16_output(o + k - off, m), m);
+        }
+        return;
+    }
+    const uint32_t d = static_cast<uint32_t>(off);
+    const uint4 v = lzw::ld16_output(o - d, d);
+    uint32_t u[4] = {0, 0, 0, 0};
+    uint32_t k = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < 16; ++j) {
+        u[j >> 2] |= lzw::byte_of(v, k) << ((j & 3) * 8);
+        k = k + 1 == d ? 0 : k + 1;
+    }
+    const uint4 uv = make_uint4(u[0], u[1], u[2], u[3]);
+    const uint32_t P = d * (16 / d);
+    for (uint64_t x = 0; x < n; x += P)
+        lzw::st16_global(o + x, uv, n - x < P ? static_cast<uint32_t>(n - x) : P);
 }
 
 // Decode one frame; every lane returns the same status and *written.
@@ -122,6 +215,7 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
     for (;;) {
         if (N - pos < 3) return CUDEC_ERR_CORRUPT_INPUT;
         const uint32_t raw = static_cast<uint32_t>(rd_le(f + pos, 3));
+        ZS_EV(0, 1);
         const bool last = raw & 1;
         const unsigned btype = (raw >> 1) & 3;
         const uint32_t bsize = raw >> 3;
@@ -163,6 +257,7 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                 streams = lfmt == 0 ? 1 : 4;
             }
             if (regen > bmax) return CUDEC_ERR_CORRUPT_INPUT;
+            ZS_T(t_lit);
             const uint64_t after = body - lhs;
             const uint8_t* lit_src = nullptr;  // literal bytes (input or workspace)
             uint8_t lit_byte = 0;              // RLE literals
@@ -193,6 +288,7 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                     return CUDEC_ERR_CORRUPT_INPUT;
                 }
                 if (psize == 0) return CUDEC_ERR_CORRUPT_INPUT;
+                ZS_T(t_huf);
                 bool ok;
                 if (streams == 1) {
                     bool mine = true;
@@ -218,9 +314,13 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                 }
                 if (!ok) return CUDEC_ERR_CORRUPT_INPUT;
                 __syncwarp();
+                ZS_ADD(1, t_huf);
+                ZS_EV(2, regen);
+                ZS_EV(3, streams);
                 lit_src = litbuf;
                 lused = lhs + csize;
             }
+            ZS_ADD(0, t_lit);
             // ---- sequences section (src/zstd_seq.h:320-676) ---------------
             const uint8_t* sec = b + lused;
             uint64_t rem = body - lused;
@@ -248,6 +348,7 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                 const unsigned mode[3] = {(modes >> 6) & 3, (modes >> 4) & 3, (modes >> 2) & 3};
                 sec += cnum;
                 rem -= cnum;
+                ZS_T(t_tab);
                 for (unsigned fld = 0; fld < 3; ++fld) {
                     uint64_t u;
                     if (!seq_table(w, t, fld, mode[fld], sec, rem, &u, lane))
@@ -255,6 +356,8 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                     sec += u;
                     rem -= u;
                 }
+                ZS_ADD(2, t_tab);
+                ZS_EV(1, nseq);
                 if (rem == 0) return CUDEC_ERR_CORRUPT_INPUT;
                 BitIn r;
                 if (!r.start(sec, rem)) return CUDEC_ERR_CORRUPT_INPUT;
@@ -268,6 +371,7 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                 sml = static_cast<uint32_t>(v);
                 uint64_t cur = out;   // output position including this batch
                 for (uint32_t i0 = 0; i0 < nseq; i0 += 32) {
+                    ZS_T(t_dec);
                     const uint32_t cnt = nseq - i0 < 32 ? nseq - i0 : 32;
                     // my sequence of this batch
                     uint64_t m_o = 0, m_ll = 0, m_lsrc = 0, m_off = 0, m_ml = 0;
@@ -350,15 +454,26 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                         cur += ml;
                     }
                     if (exec != CUDEC_OK) continue;  // keep decoding for stream faults
+                    ZS_ADD(3, t_dec);
+                    ZS_T(t_exe);
                     // ---- execute the batch ---------------------------------
-                    if (m_has && m_ll) {
-                        if (ltype == 1) {
-                            for (uint64_t j = 0; j < m_ll; ++j) dst[m_o + j] = lit_byte;
-                        } else {
-                            copy_bytes(dst + m_o, lit_src + m_lsrc, m_ll);
-                        }
+                    // literal runs: short ones per lane, long ones by the warp
+                    const bool lit_long = m_has && m_ll > kLaneCopyMax;
+                    if (m_has && m_ll && !lit_long) {
+                        if (ltype == 1) lane_fill(dst + m_o, lit_byte, m_ll);
+                        else lane_copy(dst + m_o, lit_src + m_lsrc, m_ll);
+                    }
+                    for (unsigned lm = __ballot_sync(0xffffffffu, lit_long); lm; lm &= lm - 1) {
+                        const int l = __ffs(lm) - 1;
+                        const uint64_t o = __shfl_sync(0xffffffffu, m_o, l);
+                        const uint64_t n = __shfl_sync(0xffffffffu, m_ll, l);
+                        const uint64_t sr = __shfl_sync(0xffffffffu, m_lsrc, l);
+                        if (ltype == 1) warp_fill(dst + o, lit_byte, n, lane);
+                        else warp_copy(dst + o, lit_src + sr, n, lane);
                     }
                     __syncwarp();
+                    // matches in frontier rounds: a match goes once every byte
+                    // its source reads lies below the lowest pending start
                     bool pend = m_has && m_ml != 0;
                     const uint64_t ms = m_o + m_ll;
                     while (__any_sync(0xffffffffu, pend)) {
@@ -366,12 +481,22 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                         const uint64_t s0 = ms - m_off;
                         const uint64_t send = s0 + m_ml < ms ? s0 + m_ml : ms;
                         const bool ready = pend && (ms == F || send <= F);
-                        if (ready) {
-                            for (uint64_t j = 0; j < m_ml; ++j) dst[ms + j] = dst[s0 + j];
+                        if (ready && m_ml <= kLaneCopyMax) {
+                            lane_match(dst, ms, m_ml, m_off);
                             pend = false;
+                        }
+                        for (unsigned lm = __ballot_sync(0xffffffffu, ready && pend); lm;
+                             lm &= lm - 1) {
+                            const int l = __ffs(lm) - 1;
+                            lzw::coop_match(dst, __shfl_sync(0xffffffffu, ms, l),
+                                            __shfl_sync(0xffffffffu, m_ml, l),
+                                            static_cast<uint32_t>(__shfl_sync(0xffffffffu, m_off, l)),
+                                            w.period, lane);
+                            if (lane == static_cast<uint32_t>(l)) pend = false;
                         }
                         __syncwarp();
                     }
+                    ZS_ADD(4, t_exe);
                 }
                 if (r.left != 0) return CUDEC_ERR_CORRUPT_INPUT;
                 if (exec != CUDEC_OK) return exec;
@@ -394,7 +519,9 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
         if (N - pos < 4) return CUDEC_ERR_CORRUPT_INPUT;
         __syncwarp();
         uint32_t h = 0;
+        ZS_T(t_ck);
         if (lane == 0) h = static_cast<uint32_t>(xxh64_dev(dst, out));
+        ZS_ADD(6, t_ck);
         h = __shfl_sync(0xffffffffu, h, 0);
         if (h != static_cast<uint32_t>(rd_le(f + pos, 4))) return CUDEC_ERR_CORRUPT_INPUT;
         pos += 4;

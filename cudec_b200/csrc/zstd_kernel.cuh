@@ -47,6 +47,7 @@ struct __align__(16) WarpSmem {
     int16_t counts[64];
     uint16_t next[64];
     uint8_t weights[260];
+    uint8_t period[512];     // a short match period staged for a warp copy
 };
 
 __device__ __forceinline__ unsigned hibit32(uint32_t v) { return 31u - __clz(v); }
@@ -66,7 +67,26 @@ struct BitIn {
     uint32_t n;        // valid bits in c
     uint64_t left;     // bits remaining in the stream
 
+    // Tops the container up to at least 57 bits (or the stream's end). With
+    // eight bytes behind the cursor it takes every whole byte that fits in
+    // one step: the 8 bytes ending at pos, read as a little-endian word (byte
+    // pos on top) from the two aligned 8-byte blocks that hold them - each
+    // block holds a requested byte, so no load leaves the stream's blocks.
     __device__ __forceinline__ void refill() {
+        if (n > 56 || pos < 0) return;
+        if (pos >= 7) {
+            const uint32_t b = (64 - n) >> 3;  // 1..8 whole bytes fit
+            const uintptr_t a = reinterpret_cast<uintptr_t>(src + pos - 7);
+            const uint32_t mis = static_cast<uint32_t>(a & 7);
+            const uint64_t* blk = reinterpret_cast<const uint64_t*>(a - mis);
+            uint64_t x = blk[0];
+            if (mis) x = (x >> (8 * mis)) | (blk[1] << (64 - 8 * mis));
+            const uint64_t top = b == 8 ? x : (x >> (64 - 8 * b)) << (64 - 8 * b);
+            c |= top >> n;
+            n += 8 * b;
+            pos -= b;
+            return;
+        }
         while (n <= 56 && pos >= 0) {
             c |= static_cast<uint64_t>(src[pos]) << (56 - n);
             n += 8;
@@ -86,6 +106,12 @@ struct BitIn {
         refill();
         return true;
     }
+    // At least k (<= 57) bits buffered, or all that remain (bits past the
+    // stream's end read as zeros).
+    __device__ __forceinline__ void ensure(uint32_t k) {
+        if (n < k) refill();
+    }
+    // The next k bits; needs ensure(k) first.
     __device__ __forceinline__ uint32_t peek(uint32_t k) const {
         return k ? static_cast<uint32_t>(c >> (64 - k)) : 0u;
     }
@@ -96,11 +122,11 @@ struct BitIn {
             return true;
         }
         if (k > left) return false;
+        ensure(k);
         *v = c >> (64 - k);
         c <<= k;
         n -= k;
         left -= k;
-        refill();
         return true;
     }
 };
@@ -394,6 +420,7 @@ __device__ inline bool huf_stream(const uint8_t* src, uint64_t size, const uint1
     BitIn r;
     if (!r.start(src, size)) return false;
     for (uint64_t i = 0; i < count; ++i) {
+        r.ensure(tl);
         const uint16_t cell = huf[r.peek(tl)];
         uint64_t b;
         if (!r.read(cell >> 8, &b)) return false;
@@ -474,9 +501,6 @@ __device__ inline bool seq_table(WarpSmem& w, Tables& t, unsigned field, unsigne
     return true;
 }
 
-__device__ __forceinline__ void copy_bytes(uint8_t* dst, const uint8_t* src, uint64_t n) {
-    for (uint64_t i = 0; i < n; ++i) dst[i] = src[i];
-}
 
 
 }  // namespace zstd
