@@ -10,6 +10,10 @@
 // decodes and reads back wave w; host-side output comes back as one copy of
 // the wave's staging into pinned memory and is scattered to the caller's
 // buffers (exactly bytes_written each) while the next wave is on the device.
+// When every compressed chunk of a call lies in page-locked host memory mapped
+// for the device, no staging happens at all: the decode kernel reads the
+// chunks over the host link itself, so the transfer overlaps the decode.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -64,6 +68,65 @@ cudec_status validate(const void* const* src, const size_t* sizes, void* const* 
     return CUDEC_OK;
 }
 
+// cuPointerGetAttribute through the runtime's driver entry point (the library
+// does not link libcuda); null when the driver does not offer it.
+using PtrAttrFn = CUresult (*)(void*, CUpointer_attribute, CUdeviceptr);
+
+PtrAttrFn ptr_attr() {
+    static const PtrAttrFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuPointerGetAttribute", &f, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            (void)cudaGetLastError();
+            return static_cast<PtrAttrFn>(nullptr);
+        }
+        return reinterpret_cast<PtrAttrFn>(f);
+    }();
+    return fn;
+}
+
+// The page-locked host allocation holding `p`, when it is mapped into the
+// current context at the same address (unified addressing): [lo, hi).
+bool pinned_range(const void* p, uintptr_t* lo, uintptr_t* hi) {
+    const PtrAttrFn get = ptr_attr();
+    if (get == nullptr) return false;
+    const CUdeviceptr a = reinterpret_cast<CUdeviceptr>(p);
+    unsigned int type = 0;
+    CUdeviceptr dev = 0, start = 0;
+    size_t span = 0;
+    if (get(&type, CU_POINTER_ATTRIBUTE_MEMORY_TYPE, a) != CUDA_SUCCESS ||
+        type != CU_MEMORYTYPE_HOST ||
+        get(&dev, CU_POINTER_ATTRIBUTE_DEVICE_POINTER, a) != CUDA_SUCCESS || dev != a ||
+        get(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, a) != CUDA_SUCCESS ||
+        get(&span, CU_POINTER_ATTRIBUTE_RANGE_SIZE, a) != CUDA_SUCCESS || span == 0 ||
+        start > a || a - start >= span)
+        return false;
+    *lo = static_cast<uintptr_t>(start);
+    *hi = static_cast<uintptr_t>(start) + span;
+    return true;
+}
+
+// True when the device can read every chunk in place: each [src, src+size)
+// inside one mapped page-locked allocation. One driver query per allocation
+// met (the last range is remembered), so a packed batch costs one query.
+// The decode kernel's window fill reads whole aligned 16-byte blocks around
+// a chunk; such a block shares its page with the chunk byte it holds, and
+// page-locked allocations are locked and mapped in whole pages.
+bool device_readable(const void* const* src, const size_t* sizes, size_t n) {
+    uintptr_t lo = 0, hi = 0;
+    for (size_t i = 0; i < n; ++i) {
+        if (sizes[i] == 0) continue;
+        const uintptr_t a = reinterpret_cast<uintptr_t>(src[i]);
+        if (a < lo || a >= hi) {
+            if (!pinned_range(src[i], &lo, &hi)) return false;
+        }
+        if (sizes[i] > hi - a) return false;
+    }
+    return true;
+}
+
 }  // namespace
 
 struct cudec_stream_ctx {
@@ -107,6 +170,7 @@ cudec_status decode(cudec_stream_ctx& ctx, const void* const* src, const size_t*
     const size_t wave = choose_wave(sizes, caps, n, host_out);
     const size_t waves = (n + wave - 1) / wave;
     stamp(results, n, CUDEC_ERR_CUDA);
+    const bool in_place = device_readable(src, sizes, n);
 
     size_t max_src = 0, max_out = 0;
     for (size_t w = 0; w < waves; ++w) {
@@ -136,8 +200,10 @@ cudec_status decode(cudec_stream_ctx& ctx, const void* const* src, const size_t*
     } while (0)
     const size_t slots = waves > 1 ? 2 : 1;
     for (size_t b = 0; b < slots; ++b) {
-        GROW(ctx.p_src[b].ensure(max_src ? max_src : 1));
-        GROW(ctx.d_src[b].ensure(max_src ? max_src : 1));
+        if (!in_place) {
+            GROW(ctx.p_src[b].ensure(max_src ? max_src : 1));
+            GROW(ctx.d_src[b].ensure(max_src ? max_src : 1));
+        }
         GROW(ctx.p_meta[b].ensure(meta_bytes));
         GROW(ctx.d_meta[b].ensure(meta_bytes));
         if (host_out) {
@@ -178,7 +244,7 @@ cudec_status decode(cudec_stream_ctx& ctx, const void* const* src, const size_t*
         // Sources laid out back to back (the usual packed batch) go up in one
         // copy straight from the caller's memory: a DMA when it is pinned, a
         // driver-staged copy otherwise; no host staging pass either way.
-        bool contiguous = true;
+        bool contiguous = !in_place;
         for (size_t j = 1; j < wn && contiguous; ++j) {
             const size_t i = begin + j;
             if (sizes[i] && static_cast<const unsigned char*>(src[i]) !=
@@ -188,8 +254,12 @@ cudec_status decode(cudec_stream_ctx& ctx, const void* const* src, const size_t*
         size_t so = 0, oo = 0;
         for (size_t j = 0; j < wn; ++j) {
             const size_t i = begin + j;
-            if (sizes[i] && !contiguous) std::memcpy(ps + so, src[i], sizes[i]);
-            pm[j] = reinterpret_cast<uint64_t>(ds + so);
+            if (in_place) {
+                pm[j] = reinterpret_cast<uint64_t>(src[i]);
+            } else {
+                if (sizes[i] && !contiguous) std::memcpy(ps + so, src[i], sizes[i]);
+                pm[j] = reinterpret_cast<uint64_t>(ds + so);
+            }
             pm[wave + j] = sizes[i];
             pm[2 * wave + j] = host_out ? reinterpret_cast<uint64_t>(dout + oo)
                                         : reinterpret_cast<uint64_t>(dst[i]);
@@ -198,7 +268,8 @@ cudec_status decode(cudec_stream_ctx& ctx, const void* const* src, const size_t*
             if (host_out) oo += caps[i];
         }
         const void* up = contiguous ? src[begin] : static_cast<const void*>(ps);
-        if (so && cudaMemcpyAsync(ds, up, so, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+        if (!in_place && so &&
+            cudaMemcpyAsync(ds, up, so, cudaMemcpyHostToDevice, s) != cudaSuccess) {
             fail = CUDEC_ERR_CUDA;
             break;
         }
@@ -265,6 +336,13 @@ cudec_status decode(cudec_stream_ctx& ctx, const void* const* src, const size_t*
 }  // namespace
 
 extern "C" {
+
+// Library-internal probe (not part of the C ABI): 1 when the streaming
+// context would let the device read these chunks in place.
+__attribute__((visibility("default"))) int cdb_stream_reads_in_place(
+    const void* const* src, const size_t* sizes, size_t n) {
+    return (src != nullptr && sizes != nullptr && device_readable(src, sizes, n)) ? 1 : 0;
+}
 
 cudec_status cudec_stream_ctx_create(cudec_stream_ctx** out_ctx) {
     if (out_ctx == nullptr) return CUDEC_ERR_INVALID_ARGUMENT;

@@ -246,3 +246,102 @@ def test_stream_poison_latch_on_allocation_failure(cuda):
     assert ctx2.decode(sp.ctypes.data, sz.ctypes.data, dp.ctypes.data, cp.ctypes.data, 1,
                        cd.MEM_HOST, res.ctypes.data) == 0
     ctx2.close()
+
+
+def _pinned_pages(nbytes):
+    """A page-aligned numpy buffer of whole pages, page-locked and mapped
+    with cudaHostRegister (portable | mapped); unregister when done."""
+    import torch
+    page = 4096
+    pages = (nbytes + page - 1) // page
+    raw = np.zeros(pages * page + page, dtype=np.uint8)
+    off = (-raw.ctypes.data) % page
+    buf = raw[off:off + pages * page]
+    rc = torch.cuda.cudart().cudaHostRegister(buf.ctypes.data, buf.nbytes, 3)
+    assert int(rc) == 0
+    return raw, buf
+
+
+def _unpin(buf):
+    import torch
+    assert int(torch.cuda.cudart().cudaHostUnregister(buf.ctypes.data)) == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("space", [0, 1])
+def test_stream_reads_page_locked_sources_in_place(cuda, space):
+    """Chunks in page-locked host memory are read by the device in place:
+    packed in one torch pinned buffer, and scattered over two registered
+    allocations at odd offsets with the last chunk ending on the final byte
+    of its allocation. A batch with one pageable chunk is staged as before.
+    Every variant matches the oracle."""
+    import torch
+    probe = cd.lib().cdb_stream_reads_in_place
+    probe.restype = ctypes.c_int
+    probe.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]
+    raws = [raw_data(n, seed=40 + i) for i, n in enumerate([1, 777, 4096, 65536, 3, 100000])]
+    comps = [W.lz4_compress(r) for r in raws]
+    caps = [len(r) + 5 for r in raws]
+    bad = bytearray(comps[3]); bad[len(bad) // 3] ^= 0x21
+    comps.insert(0, bytes(bad)); caps.insert(0, 65536)
+    comps.insert(4, b""); caps.insert(4, 0)
+    n = len(comps)
+    want = [oracle.lz4_decode(c, k) for c, k in zip(comps, caps)]
+    sizes = np.array([len(c) for c in comps], dtype=np.uint64)
+
+    def check(src_ptrs, expect_in_place, keep):
+        assert probe(src_ptrs.ctypes.data, sizes.ctypes.data, n) == int(expect_in_place)
+        _, _, _, capa, dsts, dp, res = host_arrays(comps, caps, space, cuda)
+        ctx = cd.StreamContext()
+        st = ctx.decode(src_ptrs.ctypes.data, sizes.ctypes.data, dp.ctypes.data,
+                        capa.ctypes.data, n, space, res.ctypes.data)
+        ctx.close()
+        assert st == next(w[0] for w in want if w[0] != 0)
+        for i, (ws, wb) in enumerate(want):
+            assert res[i]["status"] == ws, i
+            if ws == 0:
+                got = dsts[i] if space == cd.MEM_HOST else dsts[i].cpu().numpy()
+                assert res[i]["bytes_written"] == len(wb)
+                assert got.tobytes()[:len(wb)] == wb
+
+    # packed in one pinned tensor
+    blob = b"".join(comps)
+    pinned = torch.empty(len(blob) + 1, dtype=torch.uint8).pin_memory()
+    pinned.numpy()[:len(blob)] = np.frombuffer(blob, dtype=np.uint8)
+    offs = np.concatenate([[0], np.cumsum(sizes[:-1])]).astype(np.uint64)
+    check(offs + np.uint64(pinned.data_ptr()), True, pinned)
+
+    # scattered over two registered allocations, odd offsets, tail at the end
+    half = n // 2
+    need_a = sum(len(c) + 3 for c in comps[:half]) + 16
+    need_b = sum(len(c) + 3 for c in comps[half:]) + 4096
+    raw_a, a = _pinned_pages(need_a)
+    raw_b, b = _pinned_pages(need_b)
+    try:
+        ptrs = []
+        pos = 1
+        for c in comps[:half]:
+            a[pos:pos + len(c)] = np.frombuffer(c, dtype=np.uint8)
+            ptrs.append(a.ctypes.data + pos)
+            pos += len(c) + 3
+        # the second allocation is filled from its end backwards
+        pos = b.nbytes
+        tail = []
+        for c in reversed(comps[half:]):
+            if c:
+                pos -= len(c)
+                b[pos:pos + len(c)] = np.frombuffer(c, dtype=np.uint8)
+            tail.append(b.ctypes.data + pos)
+            if c:
+                pos -= 5
+        ptrs += list(reversed(tail))
+        scattered = np.array(ptrs, dtype=np.uint64)
+        check(scattered, True, (a, b))
+        # one pageable chunk: staged path, same results
+        loose = np.frombuffer(comps[2], dtype=np.uint8).copy()
+        mixed = scattered.copy()
+        mixed[2] = loose.ctypes.data  # comps[2] sits in the first allocation
+        check(mixed, False, loose)
+    finally:
+        _unpin(a)
+        _unpin(b)
