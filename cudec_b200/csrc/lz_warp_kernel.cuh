@@ -3,17 +3,16 @@
 //
 // One warp owns one chunk at a time (persistent grid-stride over the batch).
 // The chunk's compressed bytes stream through a per-warp shared-memory input
-// window (kIn bytes, filled ahead of the parse by cp.async). For each parse
-// window of kPW input positions starting at a known token:
+// window (kIn bytes, filled ahead of the parse by cp.async). Tokens are
+// handled in groups of up to 32:
 //
-//   1. every lane evaluates the format's speculative `step` for its share of
-//      the positions ("where would the next token start if one started
-//      here"), and four doubling rounds turn that table into 2-, 4-, 8- and
-//      16-hop tables, so lane l finds the l-th following token in five
-//      lookups: the true token chain, 32 tokens at a time, with no serial
-//      walk;
+//   1. the group walk finds the next 32 tokens of the chain: every lane takes
+//      the format's branch-free step at two of the next 64 positions, and
+//      the chain through those positions is followed with shuffles, eight
+//      hops per branch (the uncommon token headers take a general step);
+//      lane k ends up with the k-th token's position and output offset;
 //   2. each lane runs the format's exact accept/reject ladder on its token
-//      (output position from a warp scan of the token lengths); the first
+//      (output position from the walk's running sum of lengths); the first
 //      failing or terminal token decides the chunk exactly as the serial
 //      parser would;
 //   3. tokens of at most kBig bytes execute lane-parallel through a per-warp
@@ -44,18 +43,20 @@ constexpr uint32_t kIn = 4096;               // input window per warp (bytes)
 constexpr uint32_t kInAhead = kIn - 64;      // largest fill distance past the parse
 constexpr uint32_t kBatchMax = 4096;         // largest output staged per ring batch
 constexpr uint64_t kBig = 256;               // longer tokens are copied by the whole warp
-constexpr uint32_t kPW = 1024;               // largest parse window (positions per table)
-constexpr uint32_t kLevels = 5;              // hop tables: 1, 2, 4, 8, 16 tokens
-constexpr uint32_t kExit = 0xFFFF;           // hop leaves the window
-constexpr uint32_t kWarpSmem = kRing + kIn + kLevels * kPW * 2;
+constexpr uint32_t kPW = 1024;               // largest parse reach (input bytes landed ahead)
+constexpr uint32_t kHops = 8;                // chain hops per branch in the group walk
+constexpr uint32_t kStop = ~0u;              // the group walk stops at this token
+constexpr uint32_t kRefill = 512;            // input progress between window refills
+constexpr uint32_t kWarpSmem = kRing + kIn;
 constexpr unsigned kFull = 0xffffffffu;
-constexpr uint64_t kNone = ~0ull;            // no next token (speculative step)
 static_assert(kBatchMax + 16 <= kRing, "a batch never overwrites unflushed bytes");
 
-// Per-launch (or per size bucket) shape of the decode: parse window
-// (positions per hop table, <= kPW, a multiple of 32), input fill distance
-// past the parse (pw + 64 .. kInAhead) and output bytes per ring batch
-// (<= kBatchMax). Any values in range decode identically; they only move time.
+// Per-launch (or per size bucket) shape of the decode: parse reach (input
+// bytes past a group's first token that must have landed in the window
+// before the group is walked, <= kPW, a multiple of 32), input fill
+// distance past the parse (pw + 64 .. kInAhead) and output bytes per ring
+// batch (<= kBatchMax). Any values in range decode identically; they only
+// move time.
 struct Tune {
     uint32_t pw, ahead, batch;
 };
@@ -150,62 +151,68 @@ struct Lz4 {
         return CUDEC_OK;
     }
 
-    // Speculative: where the next token starts if one starts at p (p < S),
-    // or kNone. No capacity checks; equals the exact ladder's next position
-    // for every token the ladder accepts as non-terminal.
-    __device__ __forceinline__ static uint64_t step(const In& in, uint64_t S, uint64_t p) {
-        const uint32_t tok = in.at(p);
-        uint64_t q = p + 1;
-        uint64_t lit = tok >> 4;
-        if (lit == 15) {
-            uint32_t b;
-            do {
-                if (q >= S) return kNone;
-                b = in.at(q++);
-                lit += b;
-            } while (b == 255);
-        }
-        if (lit > S - q) return kNone;
-        q += lit;
-        if (S - q < kSrcSlack) return kNone;
-        q += 2;
-        if ((tok & 15) == 15) {
-            uint32_t b;
-            do {
-                if (q >= S) return kNone;
-                b = in.at(q++);
-            } while (b == 255);
-        }
-        return q;
+    // The group walk reads token headers from the landed window only: r is a
+    // position relative to the group's first token, its window slot is
+    // (gb + r) & (kIn - 1), and e bounds what may be read (the input end or
+    // the window end, whichever comes first).
+    //
+    // Branch-free step for the common token: each length carries at most one
+    // extension byte (below 255) and the token lies well inside [0, e).
+    // Returns whether it applied; *nr (the next token) and *len (literal +
+    // match bytes) are meaningful only then. Every load is a masked window
+    // slot, so none leaves the window whatever r is. The next position does
+    // not depend on the match's extension byte, so one load latency (token
+    // and literal extension in parallel) separates consecutive tokens.
+    __device__ __forceinline__ static bool step_simple(const uint8_t* win, uint32_t gb, uint32_t e,
+                                                       uint32_t r, uint32_t* nr, uint32_t* len) {
+        const uint32_t tok = win[(gb + r) & (kIn - 1)];
+        const uint32_t b1 = win[(gb + r + 1) & (kIn - 1)];
+        const uint32_t lit0 = tok >> 4, mlc = tok & 15;
+        const bool le = lit0 == 15, me = mlc == 15;
+        const uint32_t lit = le ? 15 + b1 : lit0;
+        const uint32_t q = r + (le ? 2u : 1u) + lit;  // the offset's position
+        const uint32_t b2 = win[(gb + q + 2) & (kIn - 1)];
+        *nr = q + (me ? 3u : 2u);
+        *len = lit + (me ? 19 + b2 : mlc + 4);
+        return !(le & (b1 == 255)) & !(me & (b2 == 255)) & (q + kSrcSlack <= e);
     }
 
-    // Literal + match length of the token at p, unchecked (equal to the exact
-    // ladder's lengths for every token it accepts as non-terminal).
-    __device__ __forceinline__ static uint64_t length(const In& in, uint64_t S, uint64_t p) {
-        if (p >= S) return 0;
-        const uint32_t tok = in.at(p);
-        uint64_t q = p + 1;
-        uint64_t lit = tok >> 4;
+    // General step inside [0, e): the next token's relative position and the
+    // token's output length, or kStop when the token is not a non-terminal
+    // one whose header lies wholly inside [0, e) (the exact ladder then
+    // decides it). Equals the exact ladder's next position and lengths for
+    // every token the ladder accepts as non-terminal.
+    __device__ __forceinline__ static uint32_t walk(const uint8_t* win, uint32_t gb, uint32_t e,
+                                                    uint32_t r, uint32_t* len) {
+        if (r >= e) return kStop;
+        const uint32_t tok = win[(gb + r) & (kIn - 1)];
+        uint32_t q = r + 1;
+        uint32_t lit = tok >> 4;
         if (lit == 15) {
             uint32_t b;
             do {
-                if (q >= S) return lit;
-                b = in.at(q++);
+                if (q >= e) return kStop;
+                b = win[(gb + q) & (kIn - 1)];
+                ++q;
                 lit += b;
             } while (b == 255);
         }
-        uint64_t ml = (tok & 15) + 4;
+        if (lit > e - q) return kStop;
+        q += lit;
+        if (e - q < kSrcSlack) return kStop;
+        q += 2;
+        uint32_t ml = (tok & 15) + 4;
         if ((tok & 15) == 15) {
-            if (lit > S - q) return lit + ml;
-            q += lit + 2;
             uint32_t b;
             do {
-                if (q >= S) break;
-                b = in.at(q++);
+                if (q >= e) return kStop;
+                b = win[(gb + q) & (kIn - 1)];
+                ++q;
                 ml += b;
             } while (b == 255);
         }
-        return lit + ml;
+        *len = lit + ml;
+        return q;
     }
 
     // The token at p with d bytes already produced; cap is the capacity.
@@ -281,45 +288,48 @@ struct Snappy {
         return d == declared ? CUDEC_OK : CUDEC_ERR_CORRUPT_INPUT;
     }
 
-    // Speculative next element position if one starts at p (p < S), or kNone.
-    __device__ __forceinline__ static uint64_t step(const In& in, uint64_t S, uint64_t p) {
-        const uint32_t tag = in.at(p);
+    // Branch-free step for tags whose length is in the tag (see
+    // Lz4::step_simple). Strict bound: an element ending at e may end the
+    // input, which only the general step (with its end check) decides.
+    __device__ __forceinline__ static bool step_simple(const uint8_t* win, uint32_t gb, uint32_t e,
+                                                       uint32_t r, uint32_t* nr, uint32_t* len) {
+        const uint32_t tag = win[(gb + r) & (kIn - 1)];
+        const uint32_t kind = tag & 3, l6 = tag >> 2;
+        const uint32_t hdr = kind == 0 ? 1 : (kind == 1 ? 2 : (kind == 2 ? 3 : 5));
+        const uint32_t n = kind == 1 ? 4 + (l6 & 7) : l6 + 1;
+        *nr = r + hdr + (kind == 0 ? n : 0);
+        *len = n;
+        return !(kind == 0 && l6 >= 60) & (*nr < e);
+    }
+
+    // General step inside [0, e) (see Lz4::walk): one element per step.
+    __device__ __forceinline__ static uint32_t walk(const uint8_t* win, uint32_t gb, uint32_t e,
+                                                    uint32_t r, uint32_t* len) {
+        if (r >= e) return kStop;
+        const uint32_t tag = win[(gb + r) & (kIn - 1)];
         const uint32_t kind = tag & 3;
         if (kind == 0) {
             const uint32_t l6 = tag >> 2;
-            uint64_t hdr = 1, len = l6;
+            uint32_t hdr = 1, n = l6;
             if (l6 >= 60) {
                 const uint32_t extra = l6 - 59;
                 hdr += extra;
-                if (hdr > S - p) return kNone;
-                len = 0;
+                if (hdr > e - r) return kStop;
+                n = 0;
                 for (uint32_t i = 0; i < extra; ++i)
-                    len |= static_cast<uint64_t>(in.at(p + 1 + i)) << (8 * i);
+                    n |= static_cast<uint32_t>(win[(gb + r + 1 + i) & (kIn - 1)]) << (8 * i);
+                if (n >= e) return kStop;  // also keeps n + 1 from wrapping
             }
-            len += 1;
-            const uint64_t q = p + hdr;
-            if (len > S - q) return kNone;
-            return q + len;
+            n += 1;
+            const uint32_t q = r + hdr;
+            if (n > e - q) return kStop;
+            *len = n;
+            return q + n;
         }
-        const uint64_t hdr = kind == 1 ? 2 : (kind == 2 ? 3 : 5);
-        if (hdr > S - p) return kNone;
-        return p + hdr;
-    }
-
-    __device__ __forceinline__ static uint64_t length(const In& in, uint64_t S, uint64_t p) {
-        if (p >= S) return 0;
-        const uint32_t tag = in.at(p);
-        const uint32_t kind = tag & 3;
-        if (kind == 0) {
-            const uint32_t l6 = tag >> 2;
-            if (l6 < 60) return l6 + 1;
-            const uint32_t extra = l6 - 59;
-            uint64_t len = 0;
-            for (uint32_t i = 0; i < extra && p + 1 + i < S; ++i)
-                len |= static_cast<uint64_t>(in.at(p + 1 + i)) << (8 * i);
-            return len + 1;
-        }
-        return kind == 1 ? 4 + ((tag >> 2) & 7) : (tag >> 2) + 1;
+        const uint32_t hdr = kind == 1 ? 2 : (kind == 2 ? 3 : 5);
+        if (hdr > e - r) return kStop;
+        *len = kind == 1 ? 4 + ((tag >> 2) & 7) : (tag >> 2) + 1;
+        return r + hdr;
     }
 
     __device__ __forceinline__ static int parse(const In& in, uint64_t S,
@@ -598,54 +608,72 @@ struct Filler {
 };
 
 // ---------------------------------------------------------------------------
-// Parallel token-chain parse over a window of kPW input positions starting at
-// a known token p: tab[0][i] = where the next token starts if one starts at
-// p + i (relative to p; kExit if it leaves the window or the input, or
-// cannot be a token),
-// tab[k] = 2^k steps. Lane l then finds the l-th token after a known one in
-// five lookups.
-__device__ __forceinline__ uint32_t hop(const uint16_t* tab, uint32_t t, uint32_t lane) {
-#pragma unroll
-    for (uint32_t b = 0; b < kLevels; ++b)
-        if (((lane >> b) & 1) && t != kExit) t = tab[b * kPW + t];
-    return t;
-}
+// The group walk: the next (up to) 32 tokens of the chain from a known
+// token, every lane taking the same steps. Each lane takes the format's
+// branch-free step at two of the next 64 positions (r + lane, r + 32 +
+// lane); the chain through them is followed by shuffles, kHops hops per
+// branch. A token whose step is not the simple one goes through the general
+// step; a chain that leaves the 64 positions starts the next 64 at its
+// token. Lane k gets the k-th token's position and output offset, both
+// relative to the group's first token; cnt is the number of tokens found
+// (at least one). It reads only the landed window: gb is the window slot of
+// the first token, e the readable bound relative to it (0 when the first
+// token is not in the window: lane 0 then holds it alone and the exact
+// ladder decides it). Out of line, so that the copy code of the group is
+// compiled as if the walk were not there.
+struct Walk {
+    uint32_t myr, myo, cnt;
+};
 
 template <class F>
-__device__ __forceinline__ void build_tables(const In& in, uint64_t S, uint64_t p, uint32_t pw,
-                                             uint16_t* tab, uint32_t lane) {
-    LZW_T(t_step);
-#pragma unroll 4
-    for (uint32_t i = lane; i < pw; i += 32) {
-        const uint64_t x = p + i;
-        uint32_t v = kExit;
-        if (x < S) {
-            const uint64_t nx = F::step(in, S, x);
-            if (nx != kNone && nx < S && nx - p < pw) v = static_cast<uint32_t>(nx - p);
-        }
-        tab[i] = static_cast<uint16_t>(v);
-    }
-    __syncwarp();
-    LZW_ADD(4, t_step);
-    for (uint32_t b = 1; b < kLevels; ++b) {
-        const uint16_t* lo = tab + (b - 1) * kPW;
-        uint16_t* hi = tab + b * kPW;
-#pragma unroll 4
-        for (uint32_t i = lane; i < pw; i += 32) {
-            const uint32_t a = lo[i];
-            hi[i] = a == kExit ? kExit : lo[a];
-        }
-        __syncwarp();
-    }
-}
-
-__device__ __forceinline__ uint64_t warp_incl_scan(uint64_t v, uint32_t lane) {
+__device__ __noinline__ Walk walk_group(const uint8_t* win, uint32_t gb, uint32_t e, uint64_t p,
+                                        uint64_t S, uint32_t lane) {
+    uint32_t od = 0, myo = 0, r = 0, myr = 0, cnt = 0;
+    if (e == 0) return Walk{0, 0, 1};
+    for (;;) {
+        uint32_t n0, l0, n1, l1;
+        const bool k0 = F::step_simple(win, gb, e, r + lane, &n0, &l0);
+        const bool k1 = F::step_simple(win, gb, e, r + 32 + lane, &n1, &l1);
+        const uint32_t rel0 = k0 ? n0 - r : kStop, rel1 = k1 ? n1 - r : kStop;
+        uint32_t cur = 0;
+        bool alive = true;
+        while (alive) {
 #pragma unroll
-    for (uint32_t k = 1; k < 32; k <<= 1) {
-        const uint64_t o = __shfl_up_sync(kFull, v, k);
-        if (lane >= k) v += o;
+            for (uint32_t u = 0; u < kHops; ++u) {
+                const uint32_t a = __shfl_sync(kFull, rel0, cur & 31);
+                const uint32_t b = __shfl_sync(kFull, rel1, cur & 31);
+                const uint32_t la = __shfl_sync(kFull, l0, cur & 31);
+                const uint32_t lb = __shfl_sync(kFull, l1, cur & 31);
+                const uint32_t nx = cur < 32 ? a : b;
+                const uint32_t ln = cur < 32 ? la : lb;
+                const bool take = alive & (nx != kStop);
+                if (take & (lane == cnt)) {
+                    myr = r + cur;
+                    myo = od;
+                }
+                cnt += take ? 1u : 0u;
+                od += take ? ln : 0u;
+                alive = take & (cnt < 32) & (nx < 64);
+                cur = take ? nx : cur;
+            }
+        }
+        r += cur;
+        if (cnt >= 32) break;
+        if (cur >= 64) continue;  // the chain left the 64 positions at a token
+        // the token at r needs the general step
+        if (lane == cnt) {
+            myr = r;
+            myo = od;
+        }
+        ++cnt;
+        if (cnt >= 32 || r >= e) break;
+        uint32_t len = 0;
+        const uint32_t nr = F::walk(win, gb, e, r, &len);
+        if (nr == kStop || F::at_end(p + nr, S)) break;
+        r = nr;
+        od += len;
     }
-    return v;
+    return Walk{myr, myo, cnt};
 }
 
 // Store m (1..16) bytes of v at global p (16-byte store when aligned and whole).
@@ -815,8 +843,8 @@ struct ExecSink {
 // chunk. Returns the chunk's status; *dend is the output length on success.
 template <class F, class Sink>
 __device__ __forceinline__ int parse_chunk(const uint8_t* g, uint64_t S, uint64_t cap,
-                                           uint8_t* win, uint16_t* tab, const Tune& tn,
-                                           uint32_t lane, Sink& sink, In& in, uint64_t* dend_out) {
+                                           uint8_t* win, const Tune& tn, uint32_t lane,
+                                           Sink& sink, In& in, uint64_t* dend_out) {
     *dend_out = 0;
     uint64_t p, limit;
     int status = F::begin(g, S, cap, &p, &limit);
@@ -829,74 +857,69 @@ __device__ __forceinline__ int parse_chunk(const uint8_t* g, uint64_t S, uint64_
     fill.issue(p, p + tn.ahead, lane);
     uint64_t d = 0;  // output position of the next token
     LZW_T(t_chunk);
+    uint64_t refill_at = 0;
     for (;;) {
         LZW_T(t_land);
-        uint64_t ready = fill.land();
-        // Refill ahead of the parse; it overwrites only positions before
-        // p - 64, and those leave the window's valid range.
-        fill.issue(p, p + tn.ahead, lane);
-        in.lo = fill.low();
-        const uint64_t want = S - p < tn.pw + 64 ? S : p + tn.pw + 64;
-        if (ready < want) ready = fill.land();  // the parse jumped past the window
-        in.span = ready > in.lo ? ready - in.lo : 0;
+        if (p >= refill_at) {
+            uint64_t ready = fill.land();
+            // Refill ahead of the parse; it overwrites only positions before
+            // p - 64, and those leave the window's valid range.
+            fill.issue(p, p + tn.ahead, lane);
+            in.lo = fill.low();
+            const uint64_t want = S - p < tn.pw ? S : p + tn.pw;
+            if (ready < want) ready = fill.land();  // the parse jumped past the window
+            in.span = ready > in.lo ? ready - in.lo : 0;
+            refill_at = p + kRefill;
+        }
         LZW_ADD(0, t_land);
         if (F::at_end(p, S)) {
             status = F::finish(d, limit);
             if (status == CUDEC_OK && !sink.group(Tok{}, 0, true, d)) status = CUDEC_ERR_CUDA;
             break;
         }
-        LZW_T(t_tab);
-        build_tables<F>(in, S, p, tn.pw, tab, lane);
-        LZW_ADD(1, t_tab);
-        uint32_t base = 0;
+        // ---- the next (up to) 32 tokens of the chain
+        LZW_T(t_walk);
+        const uint64_t wend = in.lo + in.span < S ? in.lo + in.span : S;
+        const uint32_t e = (p >= in.lo && p < wend) ? static_cast<uint32_t>(wend - p) : 0;
+        const Walk wk = walk_group<F>(win, static_cast<uint32_t>(gbase + p), e, p, S, lane);
+        LZW_ADD(1, t_walk);
+        LZW_T(t_grp);
+        // ---- each lane checks its token exactly; the first failing or
+        // terminal token decides the chunk as the serial parser would
+        const bool valid = lane < wk.cnt;
+        const uint64_t x = p + wk.myr;
+        const uint64_t dl = d + wk.myo;
+        Seq sq{};
+        int st = CUDEC_OK;
+        if (valid) st = F::parse(in, S, limit, x, dl, &sq);
+        uint32_t m = wk.cnt;
         bool last = false;
-        for (;;) {
-            LZW_T(t_grp);
-            // ---- the next (up to) 32 tokens of the chain, exactly checked
-            const uint32_t t = hop(tab, base, lane);
-            const bool valid = t != kExit;
-            const uint64_t x = p + t;
-            const uint64_t len = valid ? F::length(in, S, x) : 0;
-            const uint64_t dl = d + warp_incl_scan(len, lane) - len;
-            Seq sq{};
-            int st = CUDEC_OK;
-            if (valid) st = F::parse(in, S, limit, x, dl, &sq);
-            uint32_t m = __popc(__ballot_sync(kFull, valid));
-            const unsigned ev = __ballot_sync(kFull, valid && (st != CUDEC_OK || sq.done));
-            if (ev) {
-                const int e = __ffs(ev) - 1;
-                const int se = __shfl_sync(kFull, st, e);
-                if (se != CUDEC_OK) {
-                    status = se;
-                    last = true;
-                    break;
-                }
-                m = e + 1;
-                last = true;
-            }
-            const uint64_t tend = dl + sq.lit + sq.ml;
-            const uint64_t nxt = __shfl_sync(kFull, sq.next, m - 1);
-            const uint64_t dend = __shfl_sync(kFull, tend, m - 1);
-            LZW_ADD(2, t_grp);
-            LZW_EV(0, 1);
-            LZW_EV(1, m);
-            LZW_T(t_exec);
-            if (!sink.group(Tok{dl, sq.lit, sq.lit_src, sq.ml, sq.off}, m, last, dend)) {
-                status = CUDEC_ERR_CUDA;
-                last = true;
+        const unsigned ev = __ballot_sync(kFull, valid && (st != CUDEC_OK || sq.done));
+        if (ev) {
+            const int k = __ffs(ev) - 1;
+            const int se = __shfl_sync(kFull, st, k);
+            if (se != CUDEC_OK) {
+                status = se;
                 break;
             }
-            d = dend;
-            LZW_ADD(3, t_exec);
-            if (last) break;
-            if (m == 32 && nxt < S && nxt - p < tn.pw) {
-                base = static_cast<uint32_t>(nxt - p);
-                continue;
-            }
-            p = nxt;
+            m = k + 1;
+            last = true;
+        }
+        const uint64_t tend = dl + sq.lit + sq.ml;
+        const uint64_t nxt = __shfl_sync(kFull, sq.next, m - 1);
+        const uint64_t dend = __shfl_sync(kFull, tend, m - 1);
+        LZW_ADD(2, t_grp);
+        LZW_EV(0, 1);
+        LZW_EV(1, m);
+        LZW_T(t_exec);
+        if (!sink.group(Tok{dl, sq.lit, sq.lit_src, sq.ml, sq.off}, m, last, dend)) {
+            status = CUDEC_ERR_CUDA;
             break;
         }
+        d = dend;
+        LZW_ADD(3, t_exec);
         if (last) break;
+        p = nxt;
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
     LZW_ADD(5, t_chunk);
@@ -918,14 +941,14 @@ struct DirectSink {
 // the output length on success.
 template <class F>
 __device__ __forceinline__ int decode_chunk(const uint8_t* g, uint64_t S, uint8_t* dst, uint64_t cap,
-                            uint8_t* ring, uint8_t* win, uint16_t* tab, const Tune& tn,
+                            uint8_t* ring, uint8_t* win, const Tune& tn,
                             uint32_t lane, uint64_t* written) {
     *written = 0;
     In in{g, win, reinterpret_cast<uintptr_t>(g), 0, 0};
     ExecSink ex{Out{ring, dst, reinterpret_cast<uintptr_t>(dst), 0, 0}, g, dst, &in, tn, lane};
     DirectSink sink{&ex};
     uint64_t d = 0;
-    const int st = parse_chunk<F>(g, S, cap, win, tab, tn, lane, sink, in, &d);
+    const int st = parse_chunk<F>(g, S, cap, win, tn, lane, sink, in, &d);
     if (st != CUDEC_OK) return st;
     ex.finish(d);
     *written = d;
@@ -933,7 +956,7 @@ __device__ __forceinline__ int decode_chunk(const uint8_t* g, uint64_t S, uint8_
 }
 
 template <class F>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
     lz_warp_kernel(const void* const* src_ptrs, const size_t* src_sizes, void* const* dst_ptrs,
                    const size_t* dst_caps, size_t n, cudec_chunk_result* results, Tune tn) {
     extern __shared__ __align__(16) uint8_t lzw_smem[];
@@ -941,13 +964,12 @@ __global__ void __launch_bounds__(kThreads)
     uint8_t* base = lzw_smem + warp * kWarpSmem;
     uint8_t* ring = base;
     uint8_t* win = base + kRing;
-    uint16_t* tab = reinterpret_cast<uint16_t*>(base + kRing + kIn);
     const size_t total = static_cast<size_t>(gridDim.x) * kWarps;
     for (size_t c = static_cast<size_t>(blockIdx.x) * kWarps + warp; c < n; c += total) {
         uint64_t written = 0;
         const int st = decode_chunk<F>(static_cast<const uint8_t*>(src_ptrs[c]), src_sizes[c],
                                        static_cast<uint8_t*>(dst_ptrs[c]), dst_caps[c], ring,
-                                       win, tab, tn, lane, &written);
+                                       win, tn, lane, &written);
         if (lane == 0) {
             results[c].status = st;
             results[c].reserved = 0;

@@ -118,9 +118,7 @@ template <class F>
 __device__ __noinline__ int mixed_lz(const uint8_t* src, uint64_t S, uint8_t* dst, uint64_t cap,
                                      uint8_t* base, lzw::Tune tn, uint32_t lane,
                                      uint64_t* written) {
-    return lzw::decode_chunk<F>(src, S, dst, cap, base, base + lzw::kRing,
-                                reinterpret_cast<uint16_t*>(base + lzw::kRing + lzw::kIn), tn,
-                                lane, written);
+    return lzw::decode_chunk<F>(src, S, dst, cap, base, base + lzw::kRing, tn, lane, written);
 }
 
 __device__ __noinline__ int mixed_zstd(const uint8_t* src, uint64_t S, uint8_t* dst, uint64_t cap,
