@@ -49,7 +49,7 @@ constexpr uint32_t kStop = ~0u;              // the group walk stops at this tok
 constexpr uint32_t kRefill = 512;            // input progress between window refills
 constexpr uint32_t kWarpSmem = kRing + kIn;
 constexpr unsigned kFull = 0xffffffffu;
-static_assert(kBatchMax + 16 <= kRing, "a batch never overwrites unflushed bytes");
+static_assert(kBatchMax + 20 <= kRing, "a batch never overwrites unflushed bytes");
 
 // Per-launch (or per size bucket) shape of the decode: parse reach (input
 // bytes past a group's first token that must have landed in the window
@@ -466,14 +466,52 @@ struct Out {
         return make_uint4(w[0], w[1], w[2], w[3]);
     }
 
-    // Write the first m (1..16) bytes of v at output position x (ring).
+    // Write the first m (1..16) bytes of v at output position x (ring). The
+    // ring bytes of the current batch start at zero (clear()) and every byte
+    // has one writer, so the bytes are OR-ed in as (at most five) aligned
+    // words; neighbouring lanes may share the edge words.
     __device__ __forceinline__ void put16(uint64_t x, const uint4& v, uint32_t m) const {
         const uint32_t ix = idx(x);
-        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-        for (uint32_t j = 0; j < 16; ++j) {
-            if (j < m) ring[(ix + j) & (kRing - 1)] = static_cast<uint8_t>(w[j >> 2] >> ((j & 3) * 8));
+        const uint32_t sb = ix & 3, sh = 8 * sb;
+        uint64_t lo = (static_cast<uint64_t>(v.y) << 32) | v.x;
+        uint64_t hi = (static_cast<uint64_t>(v.w) << 32) | v.z;
+        if (m < 16) {
+            if (m <= 8) {
+                hi = 0;
+                if (m < 8) lo &= (1ull << (8 * m)) - 1;
+            } else {
+                hi &= (1ull << (8 * (m - 8))) - 1;
+            }
         }
+        const uint32_t w0 = static_cast<uint32_t>(lo), w1 = static_cast<uint32_t>(lo >> 32);
+        const uint32_t w2 = static_cast<uint32_t>(hi), w3 = static_cast<uint32_t>(hi >> 32);
+        const uint32_t last = (sb + m - 1) >> 2;  // last word touched, 0..4
+        uint32_t* r32 = reinterpret_cast<uint32_t*>(ring);
+        constexpr uint32_t kMask = kRing / 4 - 1;
+        const uint32_t wi = ix >> 2;
+        atomicOr(r32 + wi, w0 << sh);
+        if (last >= 1) atomicOr(r32 + ((wi + 1) & kMask), __funnelshift_l(w0, w1, sh));
+        if (last >= 2) atomicOr(r32 + ((wi + 2) & kMask), __funnelshift_l(w1, w2, sh));
+        if (last >= 3) atomicOr(r32 + ((wi + 3) & kMask), __funnelshift_l(w2, w3, sh));
+        if (last >= 4) atomicOr(r32 + ((wi + 4) & kMask), __funnelshift_l(w3, 0u, sh));
+    }
+
+    // Zero the ring bytes of output positions [b, e) (e - b <= kRing - 16)
+    // before a batch ORs its bytes in; bytes below b in the first word keep
+    // their contents, up to 3 bytes past e may be cleared too (they belong
+    // to later output, whose batch clears them again). The caller keeps vlo
+    // above every position whose slot this clears.
+    __device__ __forceinline__ void clear(uint64_t b, uint64_t e, uint32_t lane) const {
+        if (e <= b) return;
+        uint32_t* r32 = reinterpret_cast<uint32_t*>(ring);
+        constexpr uint32_t kMask = kRing / 4 - 1;
+        const uint32_t ib = idx(b);
+        const uint32_t sb = ib & 3;
+        const uint32_t w0 = ib >> 2;
+        if (lane == 0) atomicAnd(r32 + w0, (1u << (8 * sb)) - 1);
+        const uint32_t nw = static_cast<uint32_t>((e - b + sb + 3) >> 2);  // words from w0
+        for (uint32_t k = 1 + lane; k < nw; k += 32) r32[(w0 + k) & kMask] = 0;
+        __syncwarp();
     }
 
     // Copy positions [flushed, end) that are ready to the destination: the
@@ -533,17 +571,37 @@ __device__ __forceinline__ void copy_match(const Out& out, uint64_t o, uint64_t 
         }
         return;
     }
-    // Period off < 16: expand the period to a multiple P <= 16 in registers.
+    // Period off < 16: expand the period to 16 bytes in registers by
+    // doubling (a prefix of length off * 2^k repeated next to itself keeps
+    // period off), then write it every P bytes, P = the largest multiple of
+    // off up to 16.
     const uint4 v = out.fetch16(o - off, off);
-    uint32_t u[4] = {0, 0, 0, 0};
-    uint32_t k = 0;
-#pragma unroll
-    for (uint32_t j = 0; j < 16; ++j) {
-        u[j >> 2] |= byte_of(v, k) << ((j & 3) * 8);
-        k = k + 1 == off ? 0 : k + 1;
+    uint64_t lo = (static_cast<uint64_t>(v.y) << 32) | v.x;
+    uint64_t hi = (static_cast<uint64_t>(v.w) << 32) | v.z;
+    if (off < 8) {
+        lo &= (1ull << (8 * off)) - 1;
+        hi = 0;
+    } else if (off > 8) {
+        hi &= (1ull << (8 * (off - 8))) - 1;
+    } else {
+        hi = 0;
     }
-    const uint4 uv = make_uint4(u[0], u[1], u[2], u[3]);
-    const uint32_t P = off * (16 / off);
+#pragma unroll
+    for (uint32_t len = off, k = 0; k < 4; ++k, len <<= 1) {
+        if (len < 16) {  // (lo, hi) |= (lo, hi) << 8 * len
+            if (len < 8) {
+                hi |= (hi << (8 * len)) | (lo >> (64 - 8 * len));
+                lo |= lo << (8 * len);
+            } else {
+                hi |= lo << (8 * (len - 8));
+            }
+        }
+    }
+    const uint4 uv = make_uint4(static_cast<uint32_t>(lo), static_cast<uint32_t>(lo >> 32),
+                                static_cast<uint32_t>(hi), static_cast<uint32_t>(hi >> 32));
+    // P - 1 for off = 1..15, one nibble each
+    const uint32_t P =
+        static_cast<uint32_t>((0xEDCBA98FDBEFEFF0ull >> (4 * off)) & 15) + 1;
     for (uint64_t x = 0; x < n; x += P) {
         const uint32_t m = n - x < P ? static_cast<uint32_t>(n - x) : P;
         out.put16(o + x, uv, m);
@@ -760,8 +818,12 @@ __device__ __forceinline__ void coop_match(uint8_t* dst, uint64_t ms, uint64_t n
 // match of mi bytes at offset off); bend = end of the batch's output.
 __device__ __forceinline__ void exec_small(Out& out, const In& in, bool act, uint64_t o,
                                            uint64_t li, uint64_t lsrc, uint64_t mi,
-                                           uint32_t off, uint64_t bend, uint32_t lane) {
-    if (bend > out.vlo + kRing) out.vlo = bend - kRing;
+                                           uint32_t off, uint64_t bstart, uint64_t bend,
+                                           uint32_t lane) {
+    // clear() may zero up to 3 bytes past bend, whose slots held positions
+    // up to bend + 3 - kRing: those are read back from the destination.
+    if (bend + 4 > out.vlo + kRing) out.vlo = bend + 4 - kRing;
+    out.clear(bstart, bend, lane);
     const uint64_t ms = o + li;
     if (act && li) copy_literal(out, in, lsrc, o, li);
     __syncwarp();
@@ -830,7 +892,7 @@ struct ExecSink {
             }
             const uint64_t bend = __shfl_sync(kFull, tend, e - 1);
             exec_small(out, *in, act && lane >= s0 && lane < e, t.o, t.li, t.lsrc, t.mi, t.off,
-                       bend, lane);
+                       os, bend, lane);
             s0 = e;
         }
     }
