@@ -225,7 +225,7 @@ cudec_status cudec_mixed_decompress(cudec_mixed_plan* plan,
                                     cudec_chunk_result* d_results,
                                     cudec_stream_t stream);
 
-/* Autotuner: decodes the given batch once per candidate shape (parse window,
+/* Autotuner: decodes the given batch once per candidate shape (parse reach,
  * input lookahead, ring batch), bucket by bucket, timing each on the device,
  * and keeps the fastest per bucket. Synchronous; destinations and results
  * receive the normal decode. */
@@ -239,7 +239,7 @@ cudec_status cudec_mixed_plan_tune(cudec_mixed_plan* plan,
                                    cudec_chunk_result* d_results,
                                    cudec_stream_t stream);
 
-/* out_params[3*b .. 3*b+2] = parse window, lookahead, ring batch of bucket b. */
+/* out_params[3*b .. 3*b+2] = parse reach, lookahead, ring batch of bucket b. */
 cudec_status cudec_mixed_plan_get_tuning(const cudec_mixed_plan* plan,
                                          uint32_t* out_params);
 
