@@ -376,74 +376,90 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                     // my sequence of this batch
                     uint64_t m_o = 0, m_ll = 0, m_lsrc = 0, m_off = 0, m_ml = 0;
                     bool m_has = false;
+                    // Branch-light: bits are taken without per-read checks
+                    // (r.left going negative marks an over-read), table and
+                    // code faults are collected in sbad, and both are tested
+                    // once per batch, every stream fault being a reject
+                    // whatever the execution verdicts were. The first
+                    // execution verdict is kept by selects in the driver's
+                    // order; state past it is never used.
+                    bool sbad = false;
                     for (uint32_t k = 0; k < cnt; ++k) {
                         const uint32_t i = i0 + k;
-                        if (sll >= t.size[0] || sof >= t.size[1] || sml >= t.size[2])
-                            return CUDEC_ERR_CORRUPT_INPUT;
-                        const uint32_t cl_ = w.fse[0][sll], co_ = w.fse[1][sof], cm_ = w.fse[2][sml];
-                        const unsigned cl = (cl_ >> 8) & 0xff, co = (co_ >> 8) & 0xff,
-                                       cm = (cm_ >> 8) & 0xff;
-                        if (cl > 35 || co > 31 || cm > 52) return CUDEC_ERR_CORRUPT_INPUT;
-                        uint64_t eo, em, el;
-                        if (!r.read(co, &eo) || !r.read(ml_bits(cm), &em) || !r.read(ll_bits(cl), &el))
-                            return CUDEC_ERR_CORRUPT_INPUT;
-                        const uint64_t ov = (1ull << co) + eo;
-                        const uint64_t ml = kMLBase[cm] + em;
-                        const uint64_t ll = kLLBase[cl] + el;
-                        if (i + 1 < nseq) {
-                            if (!r.read(cl_ & 0xff, &v)) return CUDEC_ERR_CORRUPT_INPUT;
-                            sll = (cl_ >> 16) + static_cast<uint32_t>(v);
-                            if (!r.read(cm_ & 0xff, &v)) return CUDEC_ERR_CORRUPT_INPUT;
-                            sml = (cm_ >> 16) + static_cast<uint32_t>(v);
-                            if (!r.read(co_ & 0xff, &v)) return CUDEC_ERR_CORRUPT_INPUT;
-                            sof = (co_ >> 16) + static_cast<uint32_t>(v);
+                        sbad |= (sll >= t.size[0]) | (sof >= t.size[1]) | (sml >= t.size[2]);
+                        const uint32_t cl_ = w.fse[0][sll & (kFseCells - 1)],
+                                       co_ = w.fse[1][sof & (kFseCells - 1)],
+                                       cm_ = w.fse[2][sml & (kFseCells - 1)];
+                        unsigned cl = (cl_ >> 8) & 0xff, co = (co_ >> 8) & 0xff,
+                                 cm = (cm_ >> 8) & 0xff;
+                        sbad |= (cl > 35) | (co > 31) | (cm > 52);
+                        cl = cl > 35 ? 35 : cl;
+                        co = co > 31 ? 31 : co;
+                        cm = cm > 52 ? 52 : cm;
+                        const unsigned mlb = ml_bits(cm), llb = ll_bits(cl);
+                        const unsigned xb = co + mlb + llb;  // extra bits
+                        const bool upd = i + 1 < nseq;
+                        const unsigned lb = cl_ & 0xff, mb = cm_ & 0xff, ob = co_ & 0xff;
+                        const unsigned sb = upd ? lb + mb + ob : 0u;  // state bits
+                        uint32_t eo, em, el, ul = 0, um = 0, uo = 0;
+                        r.refill();
+                        if (static_cast<int32_t>(xb + sb) <= r.n) {
+                            // every field of the sequence from one container:
+                            // offset, match, literal extras, then the ll, ml
+                            // and of state bits, in stream order
+                            eo = r.field(0, co);
+                            em = r.field(co, mlb);
+                            el = r.field(co + mlb, llb);
+                            ul = r.field(xb, lb);
+                            um = r.field(xb + lb, mb);
+                            uo = r.field(xb + lb + mb, ob);
+                            r.skip(xb + sb);
+                        } else {  // long fields: refill between them
+                            eo = static_cast<uint32_t>(r.take(co));
+                            r.refill();
+                            em = static_cast<uint32_t>(r.take(mlb));
+                            r.refill();
+                            el = static_cast<uint32_t>(r.take(llb));
+                            if (upd) {
+                                r.refill();
+                                ul = static_cast<uint32_t>(r.take(lb));
+                                um = static_cast<uint32_t>(r.take(mb));
+                                uo = static_cast<uint32_t>(r.take(ob));
+                            }
                         }
-                        if (exec != CUDEC_OK) continue;
+                        if (upd) {
+                            sll = (cl_ >> 16) + ul;
+                            sml = (cm_ >> 16) + um;
+                            sof = (co_ >> 16) + uo;
+                        }
+                        // values fit 32 bits: a code below 32 plus its extra
+                        // bits, lengths below 2^17 + 2^16
+                        const uint32_t ov = (co == 31 ? 0x80000000u : (1u << co)) + eo;
+                        const uint32_t ml = kMLBase[cm] + em;
+                        const uint32_t ll = kLLBase[cl] + el;
                         // the driver's per-sequence checks, in its order
-                        if (lp + ll > regen) {
-                            exec = CUDEC_ERR_CORRUPT_INPUT;
-                            continue;
-                        }
+                        const bool bad_lit = lp + ll > regen;
                         const uint64_t o = cur, lsrc = lp;
-                        lp += ll;
-                        cur += ll;
-                        uint64_t off;
-                        if (ov > 3) {
-                            off = ov - 3;
-                            rep2 = rep1;
-                            rep1 = rep0;
-                            rep0 = off;
-                        } else {
-                            unsigned taken;
-                            if (ll != 0) {
-                                taken = static_cast<unsigned>(ov) - 1;
-                                off = taken == 0 ? rep0 : taken == 1 ? rep1 : rep2;
-                            } else if (ov < 3) {
-                                taken = static_cast<unsigned>(ov);
-                                off = taken == 1 ? rep1 : rep2;
-                            } else {
-                                taken = 3;
-                                off = rep0 ? rep0 - 1 : 0;
-                            }
-                            if (off == 0) {
-                                exec = CUDEC_ERR_CORRUPT_INPUT;
-                                continue;
-                            }
-                            if (taken != 0) {
-                                if (taken != 1) rep2 = rep1;
-                                rep1 = rep0;
-                                rep0 = off;
-                            }
-                        }
-                        if (off > cur || off > window) {
-                            exec = CUDEC_ERR_CORRUPT_INPUT;
-                            continue;
-                        }
-                        if (cur > cap || ml > cap - cur) {
-                            exec = CUDEC_ERR_OUTPUT_TOO_SMALL;
-                            continue;
-                        }
-                        if (lane == k) {
+                        const uint64_t cur2 = cur + ll;
+                        const bool nrep = ov > 3;
+                        const unsigned tk = ll != 0 ? ov - 1 : (ov < 3 ? ov : 3u);
+                        const uint64_t rsel = tk == 0 ? rep0 : tk == 1 ? rep1 : tk == 2 ? rep2
+                                            : (rep0 ? rep0 - 1 : 0);
+                        const uint64_t off = nrep ? static_cast<uint64_t>(ov) - 3 : rsel;
+                        const bool bad_zero = !nrep && off == 0;
+                        const bool bad_off = off > cur2 || off > window;
+                        const bool small = cur2 > cap || ml > cap - cur2;
+                        const int v = bad_lit ? CUDEC_ERR_CORRUPT_INPUT
+                                    : bad_zero ? CUDEC_ERR_CORRUPT_INPUT
+                                    : bad_off ? CUDEC_ERR_CORRUPT_INPUT
+                                    : small ? CUDEC_ERR_OUTPUT_TOO_SMALL : CUDEC_OK;
+                        const bool shift1 = nrep || tk >= 1, shift2 = nrep || tk >= 2;
+                        const uint64_t nr2 = shift2 ? rep1 : rep2;
+                        const uint64_t nr1 = shift1 ? rep0 : rep1;
+                        const uint64_t nr0 = shift1 ? off : rep0;
+                        const bool go = exec == CUDEC_OK && v == CUDEC_OK;
+                        if (exec == CUDEC_OK) exec = v;
+                        if (go && lane == k) {
                             m_o = o;
                             m_ll = ll;
                             m_lsrc = lsrc;
@@ -451,8 +467,13 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                             m_ml = ml;
                             m_has = true;
                         }
-                        cur += ml;
+                        rep2 = go ? nr2 : rep2;
+                        rep1 = go ? nr1 : rep1;
+                        rep0 = go ? nr0 : rep0;
+                        lp = go ? lp + ll : lp;
+                        cur = go ? cur2 + ml : cur;
                     }
+                    if (sbad || r.left < 0) return CUDEC_ERR_CORRUPT_INPUT;
                     if (exec != CUDEC_OK) continue;  // keep decoding for stream faults
                     ZS_ADD(3, t_dec);
                     ZS_T(t_exe);

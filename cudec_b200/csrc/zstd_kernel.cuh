@@ -40,9 +40,11 @@ constexpr int kCtaThreads = kWarpsPerCta * 32;
 constexpr uint32_t kLitSlot = 128 * 1024;   // per-warp literal buffer (block maximum)
 constexpr uint64_t kMaxWindow = 8ull << 20;
 
+constexpr uint32_t kFseCells = 512;  // FSE decode cells per field (table log <= 9)
+
 struct __align__(16) WarpSmem {
     uint16_t huf[1 << 11];   // symbol | bits << 8
-    uint32_t fse[3][512];    // next << 16 | symbol << 8 | bits
+    uint32_t fse[3][kFseCells];  // next << 16 | symbol << 8 | bits
     uint32_t wcells[64];     // Huffman-weight FSE table
     int16_t counts[64];
     uint16_t next[64];
@@ -64,8 +66,8 @@ struct BitIn {
     const uint8_t* src;
     int64_t pos;       // next byte to load (descending)
     uint64_t c;        // container, next bit at bit 63
-    uint32_t n;        // valid bits in c
-    uint64_t left;     // bits remaining in the stream
+    int32_t n;         // valid bits in c (negative once reads ran past the end)
+    int64_t left;      // bits remaining in the stream (negative: over-read)
 
     // Tops the container up to at least 57 bits (or the stream's end). With
     // eight bytes behind the cursor it takes every whole byte that fits in
@@ -75,7 +77,7 @@ struct BitIn {
     __device__ __forceinline__ void refill() {
         if (n > 56 || pos < 0) return;
         if (pos >= 7) {
-            const uint32_t b = (64 - n) >> 3;  // 1..8 whole bytes fit
+            const uint32_t b = static_cast<uint32_t>(64 - n) >> 3;  // 1..8 whole bytes fit
             const uintptr_t a = reinterpret_cast<uintptr_t>(src + pos - 7);
             const uint32_t mis = static_cast<uint32_t>(a & 7);
             const uint64_t* blk = reinterpret_cast<const uint64_t*>(a - mis);
@@ -99,9 +101,9 @@ struct BitIn {
         const uint32_t last = s[size - 1];
         if (last == 0) return false;
         const uint32_t m = hibit32(last);
-        left = (size - 1) * 8 + m;
+        left = static_cast<int64_t>((size - 1) * 8 + m);
         c = m ? (static_cast<uint64_t>(last & ((1u << m) - 1u)) << (64 - m)) : 0;
-        n = m;
+        n = static_cast<int32_t>(m);
         pos = static_cast<int64_t>(size) - 2;
         refill();
         return true;
@@ -109,7 +111,29 @@ struct BitIn {
     // At least k (<= 57) bits buffered, or all that remain (bits past the
     // stream's end read as zeros).
     __device__ __forceinline__ void ensure(uint32_t k) {
-        if (n < k) refill();
+        if (n < static_cast<int32_t>(k)) refill();
+    }
+    // Bits [s, s + k) of the container (k <= 63, s + k <= 64), unconsumed.
+    __device__ __forceinline__ uint32_t field(uint32_t s, uint32_t k) const {
+        const uint64_t x = s >= 64 ? 0ull : c << s;
+        return k ? static_cast<uint32_t>(x >> (64 - k)) : 0u;
+    }
+    // Consume k (<= 64) bits with no checks (see take).
+    __device__ __forceinline__ void skip(uint32_t k) {
+        c = k >= 64 ? 0ull : c << k;
+        n -= static_cast<int32_t>(k);
+        left -= k;
+    }
+    // The next k (<= 63) bits with no checks: the caller has at least k bits
+    // buffered or has run past the end (zeros then, and left goes negative,
+    // which the caller tests once for a whole run of reads: left only falls,
+    // so a negative total is exactly "some read wanted more than remained").
+    __device__ __forceinline__ uint64_t take(uint32_t k) {
+        const uint64_t v = k ? c >> (64 - k) : 0ull;
+        c <<= k;
+        n -= static_cast<int32_t>(k);
+        left -= k;
+        return v;
     }
     // The next k bits; needs ensure(k) first.
     __device__ __forceinline__ uint32_t peek(uint32_t k) const {
@@ -121,7 +145,7 @@ struct BitIn {
             *v = 0;
             return true;
         }
-        if (k > left) return false;
+        if (static_cast<int64_t>(k) > left) return false;
         ensure(k);
         *v = c >> (64 - k);
         c <<= k;
@@ -326,7 +350,7 @@ __device__ inline bool huf_weights(const uint8_t* src, uint64_t size, WarpSmem& 
             if (lane == 0) wt[produced] = static_cast<uint8_t>(cell >> 8);
             ++produced;
             const uint32_t nb = cell & 0xff;
-            if (nb > r.left) {
+            if (static_cast<int64_t>(nb) > r.left) {
                 if (produced == cap) return false;
                 if (oth >= tsize) return false;
                 if (lane == 0) wt[produced] = static_cast<uint8_t>(w.wcells[oth] >> 8);
@@ -417,14 +441,23 @@ __device__ inline bool huf_build(WarpSmem& w, unsigned count, unsigned tl, uint3
 // One Huffman stream of `count` symbols; writes to dst when non-null.
 __device__ inline bool huf_stream(const uint8_t* src, uint64_t size, const uint16_t* huf, unsigned tl,
                            uint8_t* dst, uint64_t count) {
+    // Five symbols per refill (5 x 11 <= 56 bits, 11 the largest table
+    // log) and no per-symbol checks: reads past the end see zeros and drive
+    // left negative, and the stream is accepted only when exactly all its
+    // bits were used, which is what the per-symbol check plus the final
+    // left == 0 of a checked decoder amount to.
     BitIn r;
     if (!r.start(src, size)) return false;
-    for (uint64_t i = 0; i < count; ++i) {
-        r.ensure(tl);
-        const uint16_t cell = huf[r.peek(tl)];
-        uint64_t b;
-        if (!r.read(cell >> 8, &b)) return false;
-        dst[i] = static_cast<uint8_t>(cell & 0xff);
+    for (uint64_t i = 0; i < count; i += 5) {
+        r.refill();
+#pragma unroll
+        for (uint32_t j = 0; j < 5; ++j) {
+            if (i + j < count) {
+                const uint16_t cell = huf[r.c >> (64 - tl)];
+                r.take(cell >> 8);
+                dst[i + j] = static_cast<uint8_t>(cell & 0xff);
+            }
+        }
     }
     return r.left == 0;
 }
