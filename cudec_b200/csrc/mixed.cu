@@ -135,7 +135,7 @@ __device__ __noinline__ int mixed_gdeflate(const uint8_t* src, uint64_t S, uint8
                             written);
 }
 
-__global__ void __launch_bounds__(kThreads) mixed_kernel(Args a) {
+__global__ void __launch_bounds__(kThreads, 2) mixed_kernel(Args a) {
     extern __shared__ __align__(16) uint8_t mixed_smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint8_t* base = mixed_smem + warp * kWarpSmem;
