@@ -814,12 +814,13 @@ __device__ __forceinline__ void coop_match(uint8_t* dst, uint64_t ms, uint64_t n
 }
 
 // Lane-parallel execution of tokens whose output fits one ring batch: each
-// active lane holds one token (literal li bytes from input lsrc to o, then a
-// match of mi bytes at offset off); bend = end of the batch's output.
+// active lane (lanes first.. of the group) holds one token (literal li bytes
+// from input lsrc to o, then a match of mi bytes at offset off); the batch's
+// output is [bstart, bend).
 __device__ __forceinline__ void exec_small(Out& out, const In& in, bool act, uint64_t o,
                                            uint64_t li, uint64_t lsrc, uint64_t mi,
                                            uint32_t off, uint64_t bstart, uint64_t bend,
-                                           uint32_t lane) {
+                                           uint32_t first, uint32_t lane) {
     // clear() may zero up to 3 bytes past bend, whose slots held positions
     // up to bend + 3 - kRing: those are read back from the destination.
     if (bend + 4 > out.vlo + kRing) out.vlo = bend + 4 - kRing;
@@ -827,19 +828,41 @@ __device__ __forceinline__ void exec_small(Out& out, const In& in, bool act, uin
     const uint64_t ms = o + li;
     if (act && li) copy_literal(out, in, lsrc, o, li);
     __syncwarp();
+    // Matches in rounds: a match copies once no unfinished match's output
+    // overlaps the bytes its source reads in this batch ([rs, re), relative
+    // to bstart; everything before bstart and every literal is written).
+    // Match starts grow with the lane, so the unfinished matches starting
+    // below re are the pending lanes among a prefix of lanes; the last of
+    // them ending by rs clears the source (the earlier ones end before it).
+    // The lowest unfinished match always clears, so every round finishes at
+    // least one.
+    // sorted by lane: tokens of earlier batches first, unused lanes last
+    const uint32_t rms = act ? static_cast<uint32_t>(ms - bstart) : (lane < first ? 0u : ~0u);
     bool pend = act && mi != 0;
-    // Each round finishes at least the pending match with the lowest start.
+    uint32_t rs = 0, re = 0;
+    if (pend) {
+        const uint64_t s0 = ms - off;
+        const uint64_t e0 = s0 + mi < ms ? s0 + mi : ms;
+        rs = s0 > bstart ? static_cast<uint32_t>(s0 - bstart) : 0u;
+        re = e0 > bstart ? static_cast<uint32_t>(e0 - bstart) : 0u;
+    }
     while (__any_sync(kFull, pend)) {
-        const uint64_t front = warp_min_u64(pend ? ms : ~0ull);
-        if (pend) {
-            const uint64_t src_end = ms - off + mi;
-            const uint64_t need = src_end < ms ? src_end : ms;
-            if (need <= front) {
-                copy_match(out, ms, mi, off);
-                pend = false;
-            }
+        const unsigned pm = __ballot_sync(kFull, pend);
+        const uint32_t rme = rms + static_cast<uint32_t>(mi);  // read only for pending lanes
+        uint32_t l = 0;  // the last lane whose match starts below re
+#pragma unroll
+        for (uint32_t st = 16; st; st >>= 1) {
+            const uint32_t c = l + st;
+            if (__shfl_sync(kFull, rms, c) < re) l = c;
         }
+        const bool below = __shfl_sync(kFull, rms, 0) < re;
+        const unsigned cand = below ? pm & (l == 31 ? kFull : ((2u << l) - 1)) : 0u;
+        const uint32_t last = cand ? 31 - __clz(cand) : 0u;
+        const uint32_t last_end = __shfl_sync(kFull, rme, last);
+        const bool ready = pend && (re <= rs || cand == 0 || last_end <= rs);
+        if (ready) copy_match(out, ms, mi, off);
         __syncwarp();
+        pend = pend && !ready;
         LZW_EV(2, 1);
     }
     out.flush(bend, false, lane);
@@ -892,7 +915,7 @@ struct ExecSink {
             }
             const uint64_t bend = __shfl_sync(kFull, tend, e - 1);
             exec_small(out, *in, act && lane >= s0 && lane < e, t.o, t.li, t.lsrc, t.mi, t.off,
-                       os, bend, lane);
+                       os, bend, s0, lane);
             s0 = e;
         }
     }
