@@ -75,15 +75,6 @@ __device__ inline uint64_t xxh64_dev(const uint8_t* p, uint64_t n) {
     return h;
 }
 
-__device__ __forceinline__ uint64_t warp_min64(uint64_t v) {
-#pragma unroll
-    for (int d = 16; d; d >>= 1) {
-        const uint64_t o = __shfl_xor_sync(0xffffffffu, v, d);
-        v = o < v ? o : v;
-    }
-    return v;
-}
-
 // Copies and fills. Sources are read with ordinary (coherent) loads: literal
 // bytes in the workspace and match sources in the destination were written
 // by this warp earlier in the same launch. A 16-byte window of a source is
@@ -493,15 +484,40 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                         else warp_copy(dst + o, lit_src + sr, n, lane);
                     }
                     __syncwarp();
-                    // matches in frontier rounds: a match goes once every byte
-                    // its source reads lies below the lowest pending start
+                    // matches in rounds: a match goes once no unfinished
+                    // match's output overlaps the bytes its source reads in
+                    // this batch ([rs, re), relative to the batch start b0;
+                    // earlier output and every literal are written). Match
+                    // starts grow with the lane, so the unfinished matches
+                    // starting below re are the pending lanes among a prefix
+                    // of lanes, and the last of them ending by rs clears the
+                    // source. The lowest unfinished match always clears.
                     bool pend = m_has && m_ml != 0;
                     const uint64_t ms = m_o + m_ll;
-                    while (__any_sync(0xffffffffu, pend)) {
-                        const uint64_t F = warp_min64(pend ? ms : ~0ull);
+                    const uint64_t b0 = __shfl_sync(0xffffffffu, m_o, 0);
+                    const uint32_t rms = m_has ? static_cast<uint32_t>(ms - b0) : ~0u;
+                    const uint32_t rme = rms + static_cast<uint32_t>(m_ml);
+                    uint32_t rs = 0, re = 0;
+                    if (pend) {
                         const uint64_t s0 = ms - m_off;
-                        const uint64_t send = s0 + m_ml < ms ? s0 + m_ml : ms;
-                        const bool ready = pend && (ms == F || send <= F);
+                        const uint64_t e0 = s0 + m_ml < ms ? s0 + m_ml : ms;
+                        rs = s0 > b0 ? static_cast<uint32_t>(s0 - b0) : 0u;
+                        re = e0 > b0 ? static_cast<uint32_t>(e0 - b0) : 0u;
+                    }
+                    while (__any_sync(0xffffffffu, pend)) {
+                        const unsigned pm = __ballot_sync(0xffffffffu, pend);
+                        uint32_t l = 0;  // the last lane whose match starts below re
+#pragma unroll
+                        for (uint32_t st = 16; st; st >>= 1) {
+                            const uint32_t c = l + st;
+                            if (__shfl_sync(0xffffffffu, rms, c) < re) l = c;
+                        }
+                        const bool below = __shfl_sync(0xffffffffu, rms, 0) < re;
+                        const unsigned cand =
+                            below ? pm & (l == 31 ? 0xffffffffu : ((2u << l) - 1)) : 0u;
+                        const uint32_t last = cand ? 31 - __clz(cand) : 0u;
+                        const uint32_t last_end = __shfl_sync(0xffffffffu, rme, last);
+                        const bool ready = pend && (re <= rs || cand == 0 || last_end <= rs);
                         if (ready && m_ml <= kLaneCopyMax) {
                             lane_match(dst, ms, m_ml, m_off);
                             pend = false;
