@@ -18,9 +18,9 @@
 //   3. tokens of at most kBig bytes execute lane-parallel through a per-warp
 //      output ring (kRing bytes, indexed by destination address mod kRing,
 //      so ring blocks and destination blocks share alignment): literal runs
-//      first, then matches in frontier rounds (a lane copies once every byte
-//      its source reads lies below the lowest unfinished match start; short
-//      periods are replicated in registers); completed 16-byte blocks leave
+//      first, then matches in rounds (a lane copies once no unfinished
+//      match's output overlaps the bytes its source reads; short periods
+//      are replicated in registers); completed 16-byte blocks leave
 //      the ring as aligned, coalesced 16-byte stores. Match sources older
 //      than the ring are read back from the destination. Longer tokens are
 //      copied by the whole warp straight to the destination.
