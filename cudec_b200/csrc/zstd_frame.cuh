@@ -201,7 +201,8 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
     }
     t.huf_log = 0;
     t.huf_present = false;
-    uint64_t rep0 = 1, rep1 = 4, rep2 = 8;
+    // repeat offsets stay below the window (at most 8 MB), so 32 bits
+    uint32_t rep0 = 1, rep1 = 4, rep2 = 8;
     uint64_t pos = hsz, out = 0;
     for (;;) {
         if (N - pos < 3) return CUDEC_ERR_CORRUPT_INPUT;
@@ -329,7 +330,7 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                 nseq = static_cast<uint32_t>(sec[1]) + (static_cast<uint32_t>(sec[2]) << 8) + 0x7F00u;
                 cnum = 3;
             }
-            uint64_t lp = 0;          // literals consumed
+            uint32_t lp = 0;          // literals consumed (at most a block)
             int exec = CUDEC_OK;      // first execution verdict
             if (nseq) {
                 if (nseq > bmax / 3) return CUDEC_ERR_CORRUPT_INPUT;
@@ -365,7 +366,8 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                     ZS_T(t_dec);
                     const uint32_t cnt = nseq - i0 < 32 ? nseq - i0 : 32;
                     // my sequence of this batch
-                    uint64_t m_o = 0, m_ll = 0, m_lsrc = 0, m_off = 0, m_ml = 0;
+                    uint64_t m_o = 0;
+                    uint32_t m_ll = 0, m_lsrc = 0, m_off = 0, m_ml = 0;
                     bool m_has = false;
                     // Branch-light: bits are taken without per-read checks
                     // (r.left going negative marks an over-read), table and
@@ -430,13 +432,14 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                         const uint32_t ll = kLLBase[cl] + el;
                         // the driver's per-sequence checks, in its order
                         const bool bad_lit = lp + ll > regen;
-                        const uint64_t o = cur, lsrc = lp;
+                        const uint64_t o = cur;
+                        const uint32_t lsrc = lp;
                         const uint64_t cur2 = cur + ll;
                         const bool nrep = ov > 3;
                         const unsigned tk = ll != 0 ? ov - 1 : (ov < 3 ? ov : 3u);
-                        const uint64_t rsel = tk == 0 ? rep0 : tk == 1 ? rep1 : tk == 2 ? rep2
+                        const uint32_t rsel = tk == 0 ? rep0 : tk == 1 ? rep1 : tk == 2 ? rep2
                                             : (rep0 ? rep0 - 1 : 0);
-                        const uint64_t off = nrep ? static_cast<uint64_t>(ov) - 3 : rsel;
+                        const uint32_t off = nrep ? ov - 3 : rsel;
                         const bool bad_zero = !nrep && off == 0;
                         const bool bad_off = off > cur2 || off > window;
                         const bool small = cur2 > cap || ml > cap - cur2;
@@ -445,9 +448,9 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                                     : bad_off ? CUDEC_ERR_CORRUPT_INPUT
                                     : small ? CUDEC_ERR_OUTPUT_TOO_SMALL : CUDEC_OK;
                         const bool shift1 = nrep || tk >= 1, shift2 = nrep || tk >= 2;
-                        const uint64_t nr2 = shift2 ? rep1 : rep2;
-                        const uint64_t nr1 = shift1 ? rep0 : rep1;
-                        const uint64_t nr0 = shift1 ? off : rep0;
+                        const uint32_t nr2 = shift2 ? rep1 : rep2;
+                        const uint32_t nr1 = shift1 ? rep0 : rep1;
+                        const uint32_t nr0 = shift1 ? off : rep0;
                         const bool go = exec == CUDEC_OK && v == CUDEC_OK;
                         if (exec == CUDEC_OK) exec = v;
                         if (go && lane == k) {
