@@ -361,6 +361,10 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                 sof = static_cast<uint32_t>(v);
                 if (!r.read(t.log[2], &v)) return CUDEC_ERR_CORRUPT_INPUT;
                 sml = static_cast<uint32_t>(v);
+                // from here the stream is read by absolute position
+                BitWin bw;
+                bw.init(sec, rem);
+                int32_t bp = static_cast<int32_t>(r.left);  // at most 8 x 128 KiB bits
                 uint64_t cur = out;   // output position including this batch
                 for (uint32_t i0 = 0; i0 < nseq; i0 += 32) {
                     ZS_T(t_dec);
@@ -389,37 +393,31 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                         cl = cl > 35 ? 35 : cl;
                         co = co > 31 ? 31 : co;
                         cm = cm > 52 ? 52 : cm;
-                        const unsigned mlb = ml_bits(cm), llb = ll_bits(cl);
-                        const unsigned xb = co + mlb + llb;  // extra bits
+                        const uint32_t lcode = kLLCode[cl], mcode = kMLCode[cm];
+                        const unsigned mlb = mcode >> 24, llb = lcode >> 24;
+                        const unsigned xb = co + mlb + llb;  // extra bits, at most 63
                         const bool upd = i + 1 < nseq;
                         const unsigned lb = cl_ & 0xff, mb = cm_ & 0xff, ob = co_ & 0xff;
                         const unsigned sb = upd ? lb + mb + ob : 0u;  // state bits
-                        uint32_t eo, em, el, ul = 0, um = 0, uo = 0;
-                        r.refill();
-                        if (static_cast<int32_t>(xb + sb) <= r.n) {
-                            // every field of the sequence from one container:
-                            // offset, match, literal extras, then the ll, ml
-                            // and of state bits, in stream order
-                            eo = r.field(0, co);
-                            em = r.field(co, mlb);
-                            el = r.field(co + mlb, llb);
-                            ul = r.field(xb, lb);
-                            um = r.field(xb + lb, mb);
-                            uo = r.field(xb + lb + mb, ob);
-                            r.skip(xb + sb);
-                        } else {  // long fields: refill between them
-                            eo = static_cast<uint32_t>(r.take(co));
-                            r.refill();
-                            em = static_cast<uint32_t>(r.take(mlb));
-                            r.refill();
-                            el = static_cast<uint32_t>(r.take(llb));
-                            if (upd) {
-                                r.refill();
-                                ul = static_cast<uint32_t>(r.take(lb));
-                                um = static_cast<uint32_t>(r.take(mb));
-                                uo = static_cast<uint32_t>(r.take(ob));
-                            }
+                        // offset, match and literal extras, then the ll, ml
+                        // and of state bits, in stream order, from the top
+                        uint32_t hi, lo;
+                        bw.window(bp, &hi, &lo);
+                        const uint32_t eo = BitWin::field(hi, lo, 0, co);
+                        const uint32_t em = BitWin::field(hi, lo, co, mlb);
+                        const uint32_t el = BitWin::field(hi, lo, co + mlb, llb);
+                        uint32_t ul, um, uo;
+                        if (xb + sb <= 64) {
+                            ul = BitWin::field(hi, lo, xb, lb);
+                            um = BitWin::field(hi, lo, xb + lb, mb);
+                            uo = BitWin::field(hi, lo, xb + lb + mb, ob);
+                        } else {  // long extras: the state bits from the next window
+                            bw.window(bp - static_cast<int32_t>(xb), &hi, &lo);
+                            ul = BitWin::field(hi, lo, 0, lb);
+                            um = BitWin::field(hi, lo, lb, mb);
+                            uo = BitWin::field(hi, lo, lb + mb, ob);
                         }
+                        bp -= static_cast<int32_t>(xb + sb);
                         if (upd) {
                             sll = (cl_ >> 16) + ul;
                             sml = (cm_ >> 16) + um;
@@ -427,9 +425,9 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                         }
                         // values fit 32 bits: a code below 32 plus its extra
                         // bits, lengths below 2^17 + 2^16
-                        const uint32_t ov = (co == 31 ? 0x80000000u : (1u << co)) + eo;
-                        const uint32_t ml = kMLBase[cm] + em;
-                        const uint32_t ll = kLLBase[cl] + el;
+                        const uint32_t ov = (1u << co) + eo;
+                        const uint32_t ml = (mcode & 0xffffffu) + em;
+                        const uint32_t ll = (lcode & 0xffffffu) + el;
                         // the driver's per-sequence checks, in its order
                         const bool bad_lit = lp + ll > regen;
                         const uint64_t o = cur;
@@ -467,7 +465,7 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                         lp = go ? lp + ll : lp;
                         cur = go ? cur2 + ml : cur;
                     }
-                    if (sbad || r.left < 0) return CUDEC_ERR_CORRUPT_INPUT;
+                    if (sbad || bp < 0) return CUDEC_ERR_CORRUPT_INPUT;
                     if (exec != CUDEC_OK) continue;  // keep decoding for stream faults
                     ZS_ADD(3, t_dec);
                     ZS_T(t_exe);
@@ -538,7 +536,7 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                     }
                     ZS_ADD(4, t_exe);
                 }
-                if (r.left != 0) return CUDEC_ERR_CORRUPT_INPUT;
+                if (bp != 0) return CUDEC_ERR_CORRUPT_INPUT;
                 if (exec != CUDEC_OK) return exec;
                 out = cur;
             }

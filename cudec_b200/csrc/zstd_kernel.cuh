@@ -155,6 +155,58 @@ struct BitIn {
     }
 };
 
+// Backward bitstream read by absolute position: bits [0, bp) of the stream
+// (little-endian bit order, bit i = byte i/8 >> i%8) remain and the next
+// bits are the highest, as BitIn reads them. window() returns the 64 bits
+// below bp (bit 63 = stream bit bp - 1) as hi:lo, bits outside the stream
+// reading as zeros; field() takes k (<= 31) of them counted from the top.
+// No state but bp: a sequence's fields come from one window and bp drops by
+// their total, with no refill and no per-read checks (bp < 0 is an
+// over-read, tested by the caller).
+struct BitWin {
+    const uint8_t* s;
+    int64_t size;
+    const uint32_t* abase;  // s rounded down to a 4-byte boundary
+    uint32_t boff;          // bit offset of s within that word
+
+    __device__ __forceinline__ void init(const uint8_t* src, uint64_t n) {
+        s = src;
+        size = static_cast<int64_t>(n);
+        abase = reinterpret_cast<const uint32_t*>(reinterpret_cast<uintptr_t>(src) & ~uintptr_t{3});
+        boff = static_cast<uint32_t>(reinterpret_cast<uintptr_t>(src) & 3) * 8;
+    }
+    __device__ __forceinline__ void window(int32_t bp, uint32_t* hi, uint32_t* lo) const {
+        if (bp >= 96) {
+            // three aligned words hold the 64 bits; each holds a stream byte
+            // (the third is read only when the bits reach into it)
+            const uint32_t t = boff + static_cast<uint32_t>(bp) - 64;
+            const uint32_t* p = abase + (t >> 5);
+            const uint32_t sh = t & 31;
+            const uint32_t w0 = __ldg(p), w1 = __ldg(p + 1);
+            const uint32_t w2 = sh ? __ldg(p + 2) : 0u;
+            *lo = __funnelshift_r(w0, w1, sh);
+            *hi = __funnelshift_r(w1, w2, sh);
+            return;
+        }
+        // near (or past) the stream's start: byte by byte
+        const int64_t low = static_cast<int64_t>(bp) - 64;
+        uint64_t x = 0;
+        for (int64_t q = low >> 3; q <= (static_cast<int64_t>(bp) - 1) >> 3; ++q) {
+            if (q < 0 || q >= size) continue;
+            const int64_t at = 8 * q - low;  // byte q's bit 0 within the window, in (-8, 64)
+            const uint64_t b = s[q];
+            x |= at >= 0 ? b << at : b >> (-at);
+        }
+        *lo = static_cast<uint32_t>(x);
+        *hi = static_cast<uint32_t>(x >> 32);
+    }
+    __device__ __forceinline__ static uint32_t field(uint32_t hi, uint32_t lo, uint32_t at,
+                                                     uint32_t k) {
+        const uint32_t t = at < 32 ? __funnelshift_lc(lo, hi, at) : __funnelshift_lc(0u, lo, at - 32);
+        return __funnelshift_rc(t, 0u, 32 - k);
+    }
+};
+
 // Forward little-endian bit reader for FSE descriptions.
 struct DescIn {
     const uint8_t* src;
@@ -462,21 +514,21 @@ __device__ inline bool huf_stream(const uint8_t* src, uint64_t size, const uint1
     return r.left == 0;
 }
 
-__device__ __forceinline__ unsigned ll_bits(unsigned c) {
-    return c < 16 ? 0 : c >= 25 ? c - 19 : (c < 20 ? 1 : c < 22 ? 2 : c < 24 ? 3 : 4);
-}
-__device__ __forceinline__ unsigned ml_bits(unsigned c) {
-    return c < 32 ? 0 : c >= 43 ? c - 36
-         : (c < 36 ? 1 : c < 38 ? 2 : c < 40 ? 3 : c < 42 ? 4 : 5);
-}
-// Baselines: code c's base is the sum of 2^extra over the codes below it.
-static __constant__ uint32_t kLLBase[36] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15,
-                                     16, 18, 20, 22, 24, 28, 32, 40, 48, 64, 128, 256, 512,
-                                     1024, 2048, 4096, 8192, 16384, 32768, 65536};
-static __constant__ uint32_t kMLBase[53] = {3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18,
-                                     19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29, 30, 31, 32,
-                                     33, 34, 35, 37, 39, 41, 43, 47, 51, 59, 67, 83, 99, 131,
-                                     259, 515, 1027, 2051, 4099, 8195, 16387, 32771, 65539};
+// Baseline | extra-bit count << 24 per code, one constant read per field.
+static __constant__ uint32_t kLLCode[36] = {
+    0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15,
+    16 | 1u << 24, 18 | 1u << 24, 20 | 1u << 24, 22 | 1u << 24, 24 | 2u << 24, 28 | 2u << 24,
+    32 | 3u << 24, 40 | 3u << 24, 48 | 4u << 24, 64 | 6u << 24, 128 | 7u << 24,
+    256 | 8u << 24, 512 | 9u << 24, 1024 | 10u << 24, 2048 | 11u << 24, 4096 | 12u << 24,
+    8192 | 13u << 24, 16384 | 14u << 24, 32768 | 15u << 24, 65536 | 16u << 24};
+static __constant__ uint32_t kMLCode[53] = {
+    3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18,
+    19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29, 30, 31, 32, 33, 34,
+    35 | 1u << 24, 37 | 1u << 24, 39 | 1u << 24, 41 | 1u << 24, 43 | 2u << 24, 47 | 2u << 24,
+    51 | 3u << 24, 59 | 3u << 24, 67 | 4u << 24, 83 | 4u << 24, 99 | 5u << 24,
+    131 | 7u << 24, 259 | 8u << 24, 515 | 9u << 24, 1027 | 10u << 24, 2051 | 11u << 24,
+    4099 | 12u << 24, 8195 | 13u << 24, 16387 | 14u << 24, 32771 | 15u << 24,
+    65539 | 16u << 24};
 static __constant__ int16_t kPreLL[36] = {4, 3, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 1, 1, 1, 2, 2,
                                    2, 2, 2, 2, 2, 2, 2, 3, 2, 1, 1, 1, 1, 1, -1, -1, -1, -1};
 static __constant__ int16_t kPreOF[29] = {1, 1, 1, 1, 1, 1, 2, 2, 2, 1, 1, 1, 1, 1, 1,
