@@ -425,11 +425,6 @@ __device__ __forceinline__ uint4 ld16_output(const uint8_t* p, uint32_t m) {
     return shift32(lo, hi, mis);
 }
 
-__device__ __forceinline__ uint32_t byte_of(const uint4& v, uint32_t k) {
-    const uint32_t w = k < 4 ? v.x : k < 8 ? v.y : k < 12 ? v.z : v.w;
-    return (w >> ((k & 3) * 8)) & 0xff;
-}
-
 // Per-warp output state. Positions are byte offsets into the chunk's output.
 struct Out {
     uint8_t* ring;     // kRing bytes of shared memory

@@ -145,17 +145,36 @@ __device__ __forceinline__ void lane_match(uint8_t* dst, uint64_t ms, uint64_t n
         }
         return;
     }
+    // the period expanded to 16 bytes by doubling (a prefix of length
+    // d * 2^k next to itself keeps period d), written every P bytes, P the
+    // largest multiple of d up to 16
     const uint32_t d = static_cast<uint32_t>(off);
     const uint4 v = lzw::ld16_output(o - d, d);
-    uint32_t u[4] = {0, 0, 0, 0};
-    uint32_t k = 0;
-#pragma unroll
-    for (uint32_t j = 0; j < 16; ++j) {
-        u[j >> 2] |= lzw::byte_of(v, k) << ((j & 3) * 8);
-        k = k + 1 == d ? 0 : k + 1;
+    uint64_t lo = (static_cast<uint64_t>(v.y) << 32) | v.x;
+    uint64_t hi = (static_cast<uint64_t>(v.w) << 32) | v.z;
+    if (d < 8) {
+        lo &= (1ull << (8 * d)) - 1;
+        hi = 0;
+    } else if (d > 8) {
+        hi &= (1ull << (8 * (d - 8))) - 1;
+    } else {
+        hi = 0;
     }
-    const uint4 uv = make_uint4(u[0], u[1], u[2], u[3]);
-    const uint32_t P = d * (16 / d);
+#pragma unroll
+    for (uint32_t len = d, k = 0; k < 4; ++k, len <<= 1) {
+        if (len < 16) {
+            if (len < 8) {
+                hi |= (hi << (8 * len)) | (lo >> (64 - 8 * len));
+                lo |= lo << (8 * len);
+            } else {
+                hi |= lo << (8 * (len - 8));
+            }
+        }
+    }
+    const uint4 uv = make_uint4(static_cast<uint32_t>(lo), static_cast<uint32_t>(lo >> 32),
+                                static_cast<uint32_t>(hi), static_cast<uint32_t>(hi >> 32));
+    // P - 1 for d = 1..15, one nibble each
+    const uint32_t P = static_cast<uint32_t>((0xEDCBA98FDBEFEFF0ull >> (4 * d)) & 15) + 1;
     for (uint64_t x = 0; x < n; x += P)
         lzw::st16_global(o + x, uv, n - x < P ? static_cast<uint32_t>(n - x) : P);
 }
