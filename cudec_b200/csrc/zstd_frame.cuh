@@ -391,7 +391,7 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                     // my sequence of this batch
                     uint64_t m_o = 0;
                     uint32_t m_ll = 0, m_lsrc = 0, m_off = 0, m_ml = 0;
-                    bool m_has = false;
+                    bool m_has = false, m_zero = false;
                     // Branch-light: bits are taken without per-read checks
                     // (r.left going negative marks an over-read), table and
                     // code faults are collected in sbad, and both are tested
@@ -447,45 +447,58 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                         const uint32_t ov = (1u << co) + eo;
                         const uint32_t ml = (mcode & 0xffffffu) + em;
                         const uint32_t ll = (lcode & 0xffffffu) + el;
-                        // the driver's per-sequence checks, in its order
-                        const bool bad_lit = lp + ll > regen;
-                        const uint64_t o = cur;
-                        const uint32_t lsrc = lp;
-                        const uint64_t cur2 = cur + ll;
+                        // repeat offsets, the one serial part of the
+                        // bookkeeping (state after a faulty sequence is
+                        // never used, so it is updated unconditionally)
                         const bool nrep = ov > 3;
                         const unsigned tk = ll != 0 ? ov - 1 : (ov < 3 ? ov : 3u);
                         const uint32_t rsel = tk == 0 ? rep0 : tk == 1 ? rep1 : tk == 2 ? rep2
                                             : (rep0 ? rep0 - 1 : 0);
                         const uint32_t off = nrep ? ov - 3 : rsel;
-                        const bool bad_zero = !nrep && off == 0;
-                        const bool bad_off = off > cur2 || off > window;
-                        const bool small = cur2 > cap || ml > cap - cur2;
-                        const int v = bad_lit ? CUDEC_ERR_CORRUPT_INPUT
-                                    : bad_zero ? CUDEC_ERR_CORRUPT_INPUT
-                                    : bad_off ? CUDEC_ERR_CORRUPT_INPUT
-                                    : small ? CUDEC_ERR_OUTPUT_TOO_SMALL : CUDEC_OK;
                         const bool shift1 = nrep || tk >= 1, shift2 = nrep || tk >= 2;
-                        const uint32_t nr2 = shift2 ? rep1 : rep2;
-                        const uint32_t nr1 = shift1 ? rep0 : rep1;
-                        const uint32_t nr0 = shift1 ? off : rep0;
-                        const bool go = exec == CUDEC_OK && v == CUDEC_OK;
-                        if (exec == CUDEC_OK) exec = v;
-                        if (go && lane == k) {
-                            m_o = o;
+                        rep2 = shift2 ? rep1 : rep2;
+                        rep1 = shift1 ? rep0 : rep1;
+                        rep0 = shift1 ? off : rep0;
+                        if (lane == k) {
                             m_ll = ll;
-                            m_lsrc = lsrc;
                             m_off = off;
                             m_ml = ml;
-                            m_has = true;
+                            m_zero = !nrep && off == 0;
                         }
-                        rep2 = go ? nr2 : rep2;
-                        rep1 = go ? nr1 : rep1;
-                        rep0 = go ? nr0 : rep0;
-                        lp = go ? lp + ll : lp;
-                        cur = go ? cur2 + ml : cur;
                     }
                     if (sbad || bp < 0) return CUDEC_ERR_CORRUPT_INPUT;
                     if (exec != CUDEC_OK) continue;  // keep decoding for stream faults
+                    // Positions by warp scans and the driver's per-sequence
+                    // checks lane-parallel, each in its order; the first
+                    // failing lane's verdict is the serial decoder's first
+                    // verdict (nothing after a failure is used).
+                    m_has = lane < cnt;
+                    uint32_t lsum = m_has ? m_ll : 0u, tsum = m_has ? m_ll + m_ml : 0u;
+#pragma unroll
+                    for (uint32_t d = 1; d < 32; d <<= 1) {
+                        const uint32_t a = __shfl_up_sync(0xffffffffu, lsum, d);
+                        const uint32_t b2 = __shfl_up_sync(0xffffffffu, tsum, d);
+                        if (lane >= d) {
+                            lsum += a;
+                            tsum += b2;
+                        }
+                    }
+                    m_lsrc = lp + lsum - (m_has ? m_ll : 0u);
+                    m_o = cur + tsum - (m_has ? m_ll + m_ml : 0u);
+                    const uint64_t cur2 = m_o + m_ll;
+                    const int v = !m_has ? CUDEC_OK
+                                : static_cast<uint64_t>(m_lsrc) + m_ll > regen ? CUDEC_ERR_CORRUPT_INPUT
+                                : m_zero ? CUDEC_ERR_CORRUPT_INPUT
+                                : (m_off > cur2 || m_off > window) ? CUDEC_ERR_CORRUPT_INPUT
+                                : (cur2 > cap || m_ml > cap - cur2) ? CUDEC_ERR_OUTPUT_TOO_SMALL
+                                : CUDEC_OK;
+                    const unsigned fails = __ballot_sync(0xffffffffu, v != CUDEC_OK);
+                    if (fails) {
+                        exec = __shfl_sync(0xffffffffu, v, __ffs(fails) - 1);
+                        continue;  // keep decoding for stream faults
+                    }
+                    lp += __shfl_sync(0xffffffffu, lsum, 31);
+                    cur += __shfl_sync(0xffffffffu, tsum, 31);
                     ZS_ADD(3, t_dec);
                     ZS_T(t_exe);
                     // ---- execute the batch ---------------------------------
