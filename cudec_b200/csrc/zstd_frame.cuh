@@ -392,26 +392,27 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                     uint64_t m_o = 0;
                     uint32_t m_ll = 0, m_lsrc = 0, m_off = 0, m_ml = 0;
                     bool m_has = false, m_zero = false;
-                    // Branch-light: bits are taken without per-read checks
-                    // (r.left going negative marks an over-read), table and
-                    // code faults are collected in sbad, and both are tested
-                    // once per batch, every stream fault being a reject
-                    // whatever the execution verdicts were. The first
-                    // execution verdict is kept by selects in the driver's
-                    // order; state past it is never used.
-                    bool sbad = false;
+                    // Branch-light: each sequence's bits come from one window
+                    // at the absolute position bp with no per-read checks; bp
+                    // going negative marks an over-read, tested once per
+                    // batch (a stream fault is a reject whatever the
+                    // execution verdicts were). Only the bitstream and the
+                    // repeat offsets are serial; positions and the execution
+                    // checks follow per batch, lane-parallel.
                     for (uint32_t k = 0; k < cnt; ++k) {
                         const uint32_t i = i0 + k;
-                        sbad |= (sll >= t.size[0]) | (sof >= t.size[1]) | (sml >= t.size[2]);
+                        // States stay below their table's size and codes
+                        // within their field's range by construction: every
+                        // table comes from seq_table (symbols checked against
+                        // the field's maximum) and fse_build (a cell's next
+                        // state base + its bits is below the table size), so
+                        // the reference's per-sequence range checks cannot
+                        // fire here; the masks only keep indexes in place.
                         const uint32_t cl_ = w.fse[0][sll & (kFseCells - 1)],
                                        co_ = w.fse[1][sof & (kFseCells - 1)],
                                        cm_ = w.fse[2][sml & (kFseCells - 1)];
-                        unsigned cl = (cl_ >> 8) & 0xff, co = (co_ >> 8) & 0xff,
-                                 cm = (cm_ >> 8) & 0xff;
-                        sbad |= (cl > 35) | (co > 31) | (cm > 52);
-                        cl = cl > 35 ? 35 : cl;
-                        co = co > 31 ? 31 : co;
-                        cm = cm > 52 ? 52 : cm;
+                        const unsigned cl = (cl_ >> 8) & 0x3f, co = (co_ >> 8) & 0x1f,
+                                       cm = (cm_ >> 8) & 0x3f;
                         const uint32_t lcode = kLLCode[cl], mcode = kMLCode[cm];
                         const unsigned mlb = mcode >> 24, llb = lcode >> 24;
                         const unsigned xb = co + mlb + llb;  // extra bits, at most 63
@@ -466,7 +467,7 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                             m_zero = !nrep && off == 0;
                         }
                     }
-                    if (sbad || bp < 0) return CUDEC_ERR_CORRUPT_INPUT;
+                    if (bp < 0) return CUDEC_ERR_CORRUPT_INPUT;
                     if (exec != CUDEC_OK) continue;  // keep decoding for stream faults
                     // Positions by warp scans and the driver's per-sequence
                     // checks lane-parallel, each in its order; the first
