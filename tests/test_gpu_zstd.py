@@ -127,6 +127,49 @@ def test_mutants_match_oracle(cuda):
     assert 0 in sts and 2 in sts
 
 
+def mutate_deep(f, rng):
+    """Damage aimed past the headers: flips and byte overwrites in the last
+    three quarters of the frame (where literal and sequence sections lie),
+    short truncations, and a block spliced from elsewhere in the frame."""
+    b = bytearray(f)
+    r = rng.random()
+    lo = min(len(b) - 1, max(12, len(b) // 4))
+    if r < 0.15:
+        b = b[:len(b) - rng.randint(1, min(16, len(b) - 1))]
+    elif r < 0.3 and len(b) > 64:
+        a = rng.randrange(lo, len(b) - 8)
+        c = rng.randrange(lo, len(b) - 8)
+        n = rng.randint(1, 8)
+        b[a:a + n] = b[c:c + n]
+    elif r < 0.5:
+        for _ in range(rng.randint(1, 4)):
+            b[rng.randrange(lo, len(b))] = rng.randrange(256)
+    else:
+        for _ in range(rng.randint(1, 3)):
+            b[rng.randrange(lo, len(b))] ^= 1 << rng.randrange(8)
+    return bytes(b)
+
+
+def test_deep_mutants_match_oracle(cuda):
+    """Status parity (and bytes on success) with the oracle on ~4,000 frames
+    damaged inside their literal and sequence sections, at exact, short and
+    generous capacities: every reject the branch-light sequence decode and
+    its per-batch checks make must be the one the serial decoder makes."""
+    rng = random.Random(2024)
+    comps, caps = [], []
+    raws = corpus([300, 2000, 9000, 33000, 130000], seed=21, copy=0.6, rle=0.15)
+    for raw in raws:
+        for lvl in (1, 3, 9, 19):
+            f = W.zstd_compress(raw, lvl, 20, lvl == 9)
+            for _ in range(200):
+                comps.append(mutate_deep(f, rng))
+                caps.append(rng.choice([len(raw), len(raw) - 1, len(raw) + 100, len(raw) // 2]))
+    b, res, dst = run_batch(cuda, comps, caps)
+    check(b, res, dst, comps, caps, "deep mutants")
+    sts = {int(r["status"]) for r in res}
+    assert 0 in sts and 2 in sts and 3 in sts
+
+
 def test_bench_shape_bit_exact_and_deterministic(cuda):
     """The benchmark's chunk shape (1 MiB frames, 1 MiB window, 10% RLE runs)
     at a reduced count, decoded twice: identical bytes and statuses."""
