@@ -15,17 +15,21 @@
 //  * tables live in the warp's shared memory: Huffman (2^11 cells), the three
 //    sequence FSE tables (512/256/512 cells), kept across blocks for the
 //    treeless and repeat modes;
-//  * Huffman literals decode with one lane per stream (4 streams → 4 lanes)
+//  * Huffman literals decode with one lane per stream (4 streams -> 4 lanes)
 //    into the warp's slot of the caller's workspace; raw literals are read in
 //    place, RLE literals are a byte;
 //  * sequences decode 32 at a time (the FSE state chain is serial), each lane
-//    keeps one; the per-sequence checks run in the reference's order while
-//    decoding; then the 32 sequences execute lane-parallel: literal copies
-//    first, then match copies in rounds, a match running once its source lies
-//    below the first unfinished match of the group;
-//  * a fast 64-bit backward bit container with the reference's strictness: a
+//    keeping one, every sequence's fields taken from one 64-bit window of the
+//    bitstream at its absolute position (BitWin); positions and the
+//    reference's execution checks then run lane-parallel per batch, and the
+//    32 sequences execute lane-parallel: literal copies first, then match
+//    copies in rounds, a match running once no unfinished match's output
+//    overlaps its source;
+//  * the table descriptions and the first states are read with a checked
+//    64-bit backward bit container (BitIn) with the reference's strictness: a
 //    read of more bits than remain is a reject, a peek past the end reads
-//    zeros.
+//    zeros; the windowed reads keep that strictness by testing the position
+//    once per batch (it goes negative on an over-read).
 #pragma once
 
 #include <cstdint>
@@ -112,28 +116,6 @@ struct BitIn {
     // stream's end read as zeros).
     __device__ __forceinline__ void ensure(uint32_t k) {
         if (n < static_cast<int32_t>(k)) refill();
-    }
-    // Bits [s, s + k) of the container (k <= 63, s + k <= 64), unconsumed.
-    __device__ __forceinline__ uint32_t field(uint32_t s, uint32_t k) const {
-        const uint64_t x = s >= 64 ? 0ull : c << s;
-        return k ? static_cast<uint32_t>(x >> (64 - k)) : 0u;
-    }
-    // Consume k (<= 64) bits with no checks (see take).
-    __device__ __forceinline__ void skip(uint32_t k) {
-        c = k >= 64 ? 0ull : c << k;
-        n -= static_cast<int32_t>(k);
-        left -= k;
-    }
-    // The next k (<= 63) bits with no checks: the caller has at least k bits
-    // buffered or has run past the end (zeros then, and left goes negative,
-    // which the caller tests once for a whole run of reads: left only falls,
-    // so a negative total is exactly "some read wanted more than remained").
-    __device__ __forceinline__ uint64_t take(uint32_t k) {
-        const uint64_t v = k ? c >> (64 - k) : 0ull;
-        c <<= k;
-        n -= static_cast<int32_t>(k);
-        left -= k;
-        return v;
     }
     // The next k bits; needs ensure(k) first.
     __device__ __forceinline__ uint32_t peek(uint32_t k) const {
@@ -493,25 +475,33 @@ __device__ inline bool huf_build(WarpSmem& w, unsigned count, unsigned tl, uint3
 // One Huffman stream of `count` symbols; writes to dst when non-null.
 __device__ inline bool huf_stream(const uint8_t* src, uint64_t size, const uint16_t* huf, unsigned tl,
                            uint8_t* dst, uint64_t count) {
-    // Five symbols per refill (5 x 11 <= 56 bits, 11 the largest table
-    // log) and no per-symbol checks: reads past the end see zeros and drive
-    // left negative, and the stream is accepted only when exactly all its
-    // bits were used, which is what the per-symbol check plus the final
-    // left == 0 of a checked decoder amount to.
-    BitIn r;
-    if (!r.start(src, size)) return false;
+    // Five symbols per 64-bit window read at the absolute bit position
+    // (5 x 11 <= 55 bits, 11 the largest table log) and no per-symbol
+    // checks: reads past the stream's start see zeros and drive bp
+    // negative, and the stream is accepted only when exactly all its bits
+    // were used, which is what per-symbol checks plus a final "all bits
+    // used" check amount to.
+    if (size == 0) return false;
+    const uint32_t last = src[size - 1];
+    if (last == 0) return false;  // no padding marker
+    int32_t bp = static_cast<int32_t>((size - 1) * 8 + hibit32(last));  // size <= 128 KiB
+    BitWin bw;
+    bw.init(src, size);
     for (uint64_t i = 0; i < count; i += 5) {
-        r.refill();
+        uint32_t hi, lo;
+        bw.window(bp, &hi, &lo);
+        uint32_t at = 0;
 #pragma unroll
         for (uint32_t j = 0; j < 5; ++j) {
             if (i + j < count) {
-                const uint16_t cell = huf[r.c >> (64 - tl)];
-                r.take(cell >> 8);
+                const uint16_t cell = huf[BitWin::field(hi, lo, at, tl)];
+                at += cell >> 8;
                 dst[i + j] = static_cast<uint8_t>(cell & 0xff);
             }
         }
+        bp -= static_cast<int32_t>(at);
     }
-    return r.left == 0;
+    return bp == 0;
 }
 
 // Baseline | extra-bit count << 24 per code, one constant read per field.
