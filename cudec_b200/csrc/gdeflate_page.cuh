@@ -47,6 +47,9 @@ struct __align__(16) Tables {
     uint16_t code[320];  // canonical codes during a table build
     uint8_t lens[320];
     uint8_t plen[20];
+    // canonical-decode state after the lengths the lookup table covers
+    // (first code and symbol index at length kTabBits + 1), per table
+    int32_t lfirst, lindex, dfirst, dindex;
 };
 
 
@@ -109,7 +112,8 @@ struct Lane {
 // the table. Returns false (all lanes) when the code is over-subscribed.
 __device__ __forceinline__ bool build_code(Tables& sm, const uint8_t* lens, uint32_t n,
                                            uint16_t* tab, uint16_t* count, uint16_t* sym,
-                                           uint32_t tbits, uint32_t lane) {
+                                           uint32_t tbits, int32_t* first_out,
+                                           int32_t* index_out, uint32_t lane) {
     __syncwarp();
     bool ok = true;
     if (lane == 0) {
@@ -132,6 +136,15 @@ __device__ __forceinline__ bool build_code(Tables& sm, const uint8_t* lens, uint
             next[b] = static_cast<uint16_t>(c);
         }
         for (int b = 0; b < 16; ++b) count[b] = cnt[b];
+        // the canonical walk's first code and symbol index once it has passed
+        // the lengths the lookup table holds (they depend on the counts only)
+        int32_t f = 0, ix = 0;
+        for (uint32_t b = 1; b <= tbits; ++b) {
+            ix += cnt[b];
+            f = (f + cnt[b]) << 1;
+        }
+        *first_out = f;
+        *index_out = ix;
         for (uint32_t s = 0; s < n; ++s) {
             const uint32_t l = lens[s];
             if (l && ok) {
@@ -156,17 +169,26 @@ __device__ __forceinline__ bool build_code(Tables& sm, const uint8_t* lens, uint
     return true;
 }
 
-// Decode a code from the low bits of bb: symbol and length, or false.
+// Decode a code from the low bits of bb: symbol and length, or false. Codes
+// of up to kTabBits bits come from the lookup table; longer ones continue the
+// canonical walk at length kTabBits + 1 from the state build_code stored (a
+// zero table entry means no shorter code matched, so the walk would not have
+// stopped earlier), with the code so far the first kTabBits bits in reading
+// order.
 __device__ __forceinline__ bool decode_sym(uint64_t bb, const uint16_t* tab, const uint16_t* count,
-                                           const uint16_t* sym, uint32_t* s, uint32_t* len) {
+                                           const uint16_t* sym, int32_t first0, int32_t index0,
+                                           uint32_t* s, uint32_t* len) {
     const uint16_t e = tab[bb & ((1u << kTabBits) - 1)];
     if (e) {
         *s = e & 511;
         *len = e >> 9;
         return true;
     }
-    int code = 0, first = 0, index = 0;
-    for (int l = 1; l <= 15; ++l) {
+    int code = static_cast<int>(
+                   __brev(static_cast<uint32_t>(bb) & ((1u << kTabBits) - 1)) >> (32 - kTabBits))
+               << 1;
+    int first = first0, index = index0;
+    for (int l = kTabBits + 1; l <= 15; ++l) {
         code |= static_cast<int>((bb >> (l - 1)) & 1);
         const int c = count[l];
         if (code - c < first) {
@@ -304,7 +326,9 @@ __device__ __forceinline__ int decode_page(const uint8_t* pg, uint64_t N, uint8_
             }
             if (ln.refill(lane) != kNoEvent) return CUDEC_ERR_CORRUPT_INPUT;
             // precode: complete 7-bit table (its codes are at most 7 bits)
-            if (!build_code(sm, sm.plen, 19, sm.ptab, sm.lcount, sm.lsym, 7, lane))
+            // (the precode's walk state is not used: its codes fit its table)
+            if (!build_code(sm, sm.plen, 19, sm.ptab, sm.lcount, sm.lsym, 7, &sm.lfirst,
+                            &sm.lindex, lane))
                 return CUDEC_ERR_CORRUPT_INPUT;
             const uint32_t total = hlit + hdist;
             uint32_t have = 0;
@@ -362,9 +386,11 @@ __device__ __forceinline__ int decode_page(const uint8_t* pg, uint64_t N, uint8_
             }
             if (sm.lens[256] == 0) return CUDEC_ERR_CORRUPT_INPUT;
         }
-        if (!build_code(sm, sm.lens, hlit, sm.ltab, sm.lcount, sm.lsym, kTabBits, lane))
+        if (!build_code(sm, sm.lens, hlit, sm.ltab, sm.lcount, sm.lsym, kTabBits, &sm.lfirst,
+                        &sm.lindex, lane))
             return CUDEC_ERR_CORRUPT_INPUT;
-        if (!build_code(sm, sm.lens + hlit, hdist, sm.dtab, sm.dcount, sm.dsym, kTabBits, lane))
+        if (!build_code(sm, sm.lens + hlit, hdist, sm.dtab, sm.dcount, sm.dsym, kTabBits,
+                        &sm.dfirst, &sm.dindex, lane))
             return CUDEC_ERR_CORRUPT_INPUT;
         // ---- data rounds ----
         bool pend = false, eob = false;
@@ -374,8 +400,12 @@ __device__ __forceinline__ int decode_page(const uint8_t* pg, uint64_t N, uint8_
             const bool want_lit = !pend && !eob;
             uint32_t sym = 0, clen = 0;
             bool valid = true;
-            if (want_dist) valid = decode_sym(ln.bb, sm.dtab, sm.dcount, sm.dsym, &sym, &clen);
-            else if (want_lit) valid = decode_sym(ln.bb, sm.ltab, sm.lcount, sm.lsym, &sym, &clen);
+            if (want_dist)
+                valid = decode_sym(ln.bb, sm.dtab, sm.dcount, sm.dsym, sm.dfirst, sm.dindex, &sym,
+                                   &clen);
+            else if (want_lit)
+                valid = decode_sym(ln.bb, sm.ltab, sm.lcount, sm.lsym, sm.lfirst, sm.lindex, &sym,
+                                   &clen);
             const unsigned eobm = __ballot_sync(0xffffffffu, want_lit && valid && sym == 256);
             const uint32_t e = eobm ? __ffs(eobm) - 1 : 32;
             // a bad code stops the round at its lane if that lane would act:
