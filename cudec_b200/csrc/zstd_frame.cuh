@@ -423,20 +423,26 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                         // and of state bits, in stream order, from the top
                         uint32_t hi, lo;
                         bw.window(bp, &hi, &lo);
-                        const uint32_t eo = BitWin::field(hi, lo, 0, co);
-                        const uint32_t em = BitWin::field(hi, lo, co, mlb);
+                        // offsets below 32 need no general field(): the offset
+                        // and match extras start there, and the state fields
+                        // come from the window moved past the extras
+                        const uint32_t eo = __funnelshift_rc(hi, 0u, 32 - co);
+                        const uint32_t em =
+                            __funnelshift_rc(__funnelshift_lc(lo, hi, co), 0u, 32 - mlb);
                         const uint32_t el = BitWin::field(hi, lo, co + mlb, llb);
-                        uint32_t ul, um, uo;
+                        uint32_t h2, l2;
                         if (xb + sb <= 64) {
-                            ul = BitWin::field(hi, lo, xb, lb);
-                            um = BitWin::field(hi, lo, xb + lb, mb);
-                            uo = BitWin::field(hi, lo, xb + lb + mb, ob);
+                            h2 = xb < 32 ? __funnelshift_lc(lo, hi, xb)
+                                         : __funnelshift_lc(0u, lo, xb - 32);
+                            l2 = xb < 32 ? lo << xb : 0u;
                         } else {  // long extras: the state bits from the next window
-                            bw.window(bp - static_cast<int32_t>(xb), &hi, &lo);
-                            ul = BitWin::field(hi, lo, 0, lb);
-                            um = BitWin::field(hi, lo, lb, mb);
-                            uo = BitWin::field(hi, lo, lb + mb, ob);
+                            bw.window(bp - static_cast<int32_t>(xb), &h2, &l2);
                         }
+                        const uint32_t ul = __funnelshift_rc(h2, 0u, 32 - lb);
+                        const uint32_t um =
+                            __funnelshift_rc(__funnelshift_lc(l2, h2, lb), 0u, 32 - mb);
+                        const uint32_t uo =
+                            __funnelshift_rc(__funnelshift_lc(l2, h2, lb + mb), 0u, 32 - ob);
                         bp -= static_cast<int32_t>(xb + sb);
                         if (upd) {
                             sll = (cl_ >> 16) + ul;
