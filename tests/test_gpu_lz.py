@@ -147,6 +147,79 @@ def test_overlapping_and_long_matches(cuda, fmt):
     assert all(res["status"] == 0)
 
 
+def boundary_content(rng, n):
+    """Random literal runs and exact repeats whose lengths sit on the length
+    encodings' edges: LZ4 literal runs of 14-16, 268-271 and 524-526 bytes
+    (one, two and three extension bytes, 255 in the middle), matches of
+    18-20, 272-275 and 528-530 bytes, offsets anywhere back to 64 KiB."""
+    lits = (1, 14, 15, 16, 59, 60, 61, 268, 269, 270, 271, 524, 525, 526)
+    matches = (4, 18, 19, 20, 64, 65, 272, 273, 274, 275, 528, 529, 530)
+    out = bytearray(rng.randbytes(64))
+    while len(out) < n:
+        out += rng.randbytes(rng.choice(lits))
+        m = rng.choice(matches)
+        off = rng.randint(1, min(len(out), 65535))
+        for _ in range(m):
+            out.append(out[-off])
+    return bytes(out[:n])
+
+
+def mutate_lz(c, rng):
+    """Damage aimed at the token chain: 0xFF and 15-nibble bytes (long
+    extension runs), bit flips, two-byte offset changes, truncations and a
+    spliced span."""
+    b = bytearray(c)
+    if not b:
+        return bytes(b)
+    r = rng.random()
+    if r < 0.15:
+        return bytes(b[:rng.randrange(len(b))])
+    if r < 0.3 and len(b) > 16:
+        a, z = rng.randrange(len(b) - 8), rng.randrange(len(b) - 8)
+        n = rng.randint(1, 8)
+        b[a:a + n] = b[z:z + n]
+        return bytes(b)
+    for _ in range(rng.randint(1, 3)):
+        i = rng.randrange(len(b))
+        k = rng.random()
+        if k < 0.3:
+            b[i] = 0xFF
+        elif k < 0.5:
+            b[i] = rng.choice((0x0F, 0xF0, 0xFF, 0x00))
+        elif k < 0.7 and i + 1 < len(b):
+            b[i] = rng.randrange(256)
+            b[i + 1] = rng.randrange(256)
+        else:
+            b[i] ^= 1 << rng.randrange(8)
+    return bytes(b)
+
+
+@pytest.mark.parametrize("fmt", ["lz4", "snappy"])
+def test_walk_paths_and_deep_mutants_match_oracle(cuda, fmt):
+    """The group walk's paths - the branch-free step, extension bytes of 255,
+    tokens at the input window's edge, the general step - on content built
+    at the length encodings' edges, intact (every chunk must decode) and
+    under ~1,800 mutants at exact, short and generous capacities; status and
+    bytes must equal the oracle's."""
+    rng = random.Random(31)
+    sizes = [100, 5000, 30000, 65536, 131072, 300000]
+    raws = [boundary_content(rng, n) for n in sizes]
+    comps = [COMPRESS[fmt](r) for r in raws]
+    caps = [len(r) for r in raws]
+    b, res, dst = run_batch(cuda, fmt, comps, caps)
+    check_against_oracle(fmt, b, res, dst, comps, caps, "boundaries")
+    assert all(res["status"] == 0)
+    mcomps, mcaps = [], []
+    for r, c in zip(raws, comps):
+        for _ in range(300):
+            mcomps.append(mutate_lz(c, rng))
+            mcaps.append(rng.choice([len(r), len(r) - 1, len(r) + 100, len(r) // 2]))
+    b, res, dst = run_batch(cuda, fmt, mcomps, mcaps)
+    check_against_oracle(fmt, b, res, dst, mcomps, mcaps, "deep mutants")
+    sts = {int(x) for x in res["status"]}
+    assert 0 in sts and 2 in sts
+
+
 def test_config1_shape_bit_exact_and_deterministic(cuda):
     """1,024 x 64 KiB LZ4 chunks (the headline workload), twice."""
     raws = gen([65536] * 1024, seed=1234)
