@@ -117,6 +117,41 @@ def test_mutants_match_oracle(cuda):
     assert 0 in sts and 2 in sts
 
 
+def skewed_pages(seed):
+    """Bytes drawn from geometric distributions over all 256 values: most
+    symbols are rare, so the dynamic codes reach the 15-bit limit and the
+    decoder's path for codes longer than its lookup table is exercised."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for ratio in (0.55, 0.7, 0.8, 0.9):
+        w = ratio ** np.arange(256)
+        out.append(rng.choice(256, size=65536, p=w / w.sum()).astype(np.uint8).tobytes())
+    return out
+
+
+def test_long_codes_and_their_mutants_match_oracle(cuda):
+    """Pages whose Huffman codes run past the 10-bit lookup table, at three
+    encoder levels, intact and under mutants; status and bytes must equal
+    the oracle's."""
+    rng = random.Random(77)
+    comps, caps = [], []
+    for raw in skewed_pages(3):
+        for lvl in (1, 6, 12):
+            page = W.gdeflate_compress(raw, lvl)
+            comps.append(page)
+            caps.append(len(raw))
+            for _ in range(40):
+                m = bytearray(page)
+                for _ in range(rng.randint(1, 3)):
+                    m[rng.randrange(len(m))] ^= 1 << rng.randrange(8)
+                comps.append(bytes(m))
+                caps.append(rng.choice([len(raw), len(raw) - 5, 65536]))
+    b, res, dst = run(cuda, comps, caps)
+    check(b, res, dst, comps, caps, "long codes")
+    intact = [int(res[i]["status"]) for i in range(0, len(comps), 41)]
+    assert intact == [0] * len(intact)
+
+
 def test_tilestream_container(cuda):
     raw = b"".join(pages(17))
     ts = W.gdeflate_tilestream(raw, 6)
