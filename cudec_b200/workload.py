@@ -215,15 +215,16 @@ def zstd_version():
     return _zstdlib().ZSTD_versionNumber()
 
 
-def zstd_compress(data, level=3, window_log=20, checksum=False):
-    """One Zstd frame via libzstd ZSTD_compress2 (content size always
-    written; window log and checksum flag as given)."""
+def zstd_compress(data, level=3, window_log=20, checksum=False, content_size=True):
+    """One Zstd frame via libzstd ZSTD_compress2 (window log, checksum flag
+    and whether the frame states its content size as given)."""
     Z = _zstdlib()
     data = bytes(data)
     cctx = Z.ZSTD_createCCtx()
     try:
         for p, v in ((_ZSTD_C_LEVEL, level), (_ZSTD_C_WINDOWLOG, window_log),
-                     (_ZSTD_C_CONTENTSIZE, 1), (_ZSTD_C_CHECKSUM, 1 if checksum else 0)):
+                     (_ZSTD_C_CONTENTSIZE, 1 if content_size else 0),
+                     (_ZSTD_C_CHECKSUM, 1 if checksum else 0)):
             if Z.ZSTD_isError(Z.ZSTD_CCtx_setParameter(cctx, p, v)):
                 raise RuntimeError("ZSTD_CCtx_setParameter(%d)" % p)
         bound = Z.ZSTD_compressBound(len(data))

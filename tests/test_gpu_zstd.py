@@ -184,3 +184,16 @@ def test_bench_shape_bit_exact_and_deterministic(cuda):
     torch.cuda.synchronize()
     res2, dst2 = b.results(), b.dst_host()
     assert (res2 == res).all() and (dst2 == dst).all()
+
+
+def test_subset_refusals(cuda):
+    """Skippable frames, frames without a content size, a dictionary id and a
+    window above 8 MB are UNSUPPORTED on the device as in the oracle, next to
+    a frame that decodes."""
+    import zstd_subset
+    cases = list(zstd_subset.refused_frames().values())
+    comps = [c[0] for c in cases] + [W.zstd_compress(zstd_subset.RAW, 3)]
+    caps = [c[1] for c in cases] + [len(zstd_subset.RAW)]
+    b, res, dst = run_batch(cuda, comps, caps)
+    check(b, res, dst, comps, caps, "subset")
+    assert [int(s) for s in res["status"]] == [6] * len(cases) + [0]

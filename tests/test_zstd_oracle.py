@@ -86,3 +86,16 @@ def test_zstd_oracle_agrees_with_libzstd_on_mutants():
             st, out = oracle.zstd_decode(m, 1 << 20)
             if st == 0:
                 assert W.zstd_decompress_ref(m, 1 << 20) == out
+
+
+def test_subset_refusals_match_reference():
+    """Valid frames outside the subset (skippable, no content size, a
+    dictionary id, a 16 MB window): the oracle and the reference twin both
+    refuse them as UNSUPPORTED, while libzstd decodes those that need no
+    dictionary, so the refusal is a scope line, not a malformed input."""
+    import zstd_subset
+    for name, (frame, cap, libzstd_ok) in zstd_subset.refused_frames().items():
+        assert oracle.zstd_decode(frame, cap) == (6, b""), name
+        if oracle.ref_twin_lib() is not None:
+            assert oracle.ref_zstd_decode(frame, cap)[0] == 6, name
+        assert (W.zstd_decompress_ref(frame, cap) is not None) == libzstd_ok, name
