@@ -438,18 +438,26 @@ struct Out {
         return static_cast<uint32_t>((dbase + pos) & (kRing - 1));
     }
 
+    // 16 ring bytes at position a: the five aligned words they touch, joined
+    // by funnel shifts.
     __device__ __forceinline__ uint4 ring16(uint64_t a) const {
+        constexpr uint32_t kMask = kRing / 4 - 1;
         const uint32_t ia = idx(a);
-        const uint32_t b0 = ia & ~15u, b1 = (b0 + 16) & (kRing - 1);
-        const uint4 lo = *reinterpret_cast<const uint4*>(ring + b0);
-        const uint4 hi = *reinterpret_cast<const uint4*>(ring + b1);
-        return shift32(lo, hi, ia & 15);
+        const uint32_t wi = ia >> 2, sh = (ia & 3) * 8;
+        const uint32_t* r32 = reinterpret_cast<const uint32_t*>(ring);
+        const uint32_t w0 = r32[wi], w1 = r32[(wi + 1) & kMask], w2 = r32[(wi + 2) & kMask];
+        const uint32_t w3 = r32[(wi + 3) & kMask], w4 = r32[(wi + 4) & kMask];
+        return make_uint4(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh),
+                          __funnelshift_r(w2, w3, sh), __funnelshift_r(w3, w4, sh));
     }
 
-    // m (1..16) already-written output bytes at position a.
+    // m (1..16) already-written output bytes at position a. Outside the
+    // ring, the destination holds them: vlo <= flushed always, and they are
+    // equal only right after a token copied straight to the destination,
+    // when a source may straddle vlo with its upper bytes in the ring alone.
     __device__ __forceinline__ uint4 fetch16(uint64_t a, uint32_t m) const {
         if (a >= vlo) return ring16(a);
-        if (a + m <= vlo) return ld16_output(dst + a, m);
+        if (a + m <= flushed) return ld16_output(dst + a, m);
         uint32_t w[4] = {0, 0, 0, 0};
 #pragma unroll
         for (uint32_t j = 0; j < 16; ++j) {
@@ -560,47 +568,46 @@ __device__ __forceinline__ void copy_literal(const Out& out, const In& in, uint6
 // Output [o, o + n) = the match with offset off (out[x] = out[x - off]);
 // every source byte below o is already written.
 __device__ __forceinline__ void copy_match(const Out& out, uint64_t o, uint64_t n, uint32_t off) {
-    if (off >= 16) {
-        for (uint64_t k = 0; k < n; k += 16) {
-            const uint32_t m = n - k < 16 ? static_cast<uint32_t>(n - k) : 16u;
-            out.put16(o + k, out.fetch16(o + k - off, m), m);
+    // The first piece is one fetch and one write in every lane. With a
+    // period off < 16 the fetch holds the period alone; it is expanded to 16
+    // bytes in registers by doubling (a prefix of length off * 2^k repeated
+    // next to itself keeps period off), and every later byte repeats the one
+    // Q = off * ceil(16 / off) (16..30) bytes back, which is written by then:
+    // the rest of the match is the plain copy at distance Q.
+    const uint32_t m0 = n < 16 ? static_cast<uint32_t>(n) : 16u;
+    uint4 v = out.fetch16(o - off, off < 16 ? off : m0);
+    uint32_t d = off;
+    if (off < 16) {
+        const uint64_t lo = (static_cast<uint64_t>(v.y) << 32) | v.x;
+        const uint64_t hi = (static_cast<uint64_t>(v.w) << 32) | v.z;
+        uint64_t olo, ohi;
+        if (off <= 8) {
+            // the period in the low off bytes, doubled to 8 bytes; the next 8
+            // bytes start r = 8 mod off bytes into the period: byte j of them
+            // is byte j + r of the first 8 (j < 8 - r) or byte j + r - off
+            const uint32_t s = 8 * off;  // 8..64
+            olo = lo & (~0ull >> (64 - s));
+            olo |= s < 64 ? olo << (s & 63) : 0ull;
+            olo |= s < 32 ? olo << ((2 * s) & 63) : 0ull;
+            olo |= s < 16 ? olo << ((4 * s) & 63) : 0ull;
+            // 8 mod off for off = 1..8, one nibble each
+            const uint32_t r = static_cast<uint32_t>((0x012302000ull >> (4 * off)) & 15);
+            ohi = (olo >> (8 * r)) | (olo << ((8 * (off - r)) & 63));
+        } else {
+            // 9..15 bytes: the first 16 - off of them repeat once
+            const uint32_t s = 8 * (off - 8);  // 8..56
+            olo = lo;
+            ohi = (hi & ((1ull << s) - 1)) | (lo << s);
         }
-        return;
+        v = make_uint4(static_cast<uint32_t>(olo), static_cast<uint32_t>(olo >> 32),
+                       static_cast<uint32_t>(ohi), static_cast<uint32_t>(ohi >> 32));
+        // Q - 16 for off = 1..15, one nibble each
+        d = 16 + static_cast<uint32_t>((0xECA8642052402000ull >> (4 * off)) & 15);
     }
-    // Period off < 16: expand the period to 16 bytes in registers by
-    // doubling (a prefix of length off * 2^k repeated next to itself keeps
-    // period off), then write it every P bytes, P = the largest multiple of
-    // off up to 16.
-    const uint4 v = out.fetch16(o - off, off);
-    uint64_t lo = (static_cast<uint64_t>(v.y) << 32) | v.x;
-    uint64_t hi = (static_cast<uint64_t>(v.w) << 32) | v.z;
-    if (off < 8) {
-        lo &= (1ull << (8 * off)) - 1;
-        hi = 0;
-    } else if (off > 8) {
-        hi &= (1ull << (8 * (off - 8))) - 1;
-    } else {
-        hi = 0;
-    }
-#pragma unroll
-    for (uint32_t len = off, k = 0; k < 4; ++k, len <<= 1) {
-        if (len < 16) {  // (lo, hi) |= (lo, hi) << 8 * len
-            if (len < 8) {
-                hi |= (hi << (8 * len)) | (lo >> (64 - 8 * len));
-                lo |= lo << (8 * len);
-            } else {
-                hi |= lo << (8 * (len - 8));
-            }
-        }
-    }
-    const uint4 uv = make_uint4(static_cast<uint32_t>(lo), static_cast<uint32_t>(lo >> 32),
-                                static_cast<uint32_t>(hi), static_cast<uint32_t>(hi >> 32));
-    // P - 1 for off = 1..15, one nibble each
-    const uint32_t P =
-        static_cast<uint32_t>((0xEDCBA98FDBEFEFF0ull >> (4 * off)) & 15) + 1;
-    for (uint64_t x = 0; x < n; x += P) {
-        const uint32_t m = n - x < P ? static_cast<uint32_t>(n - x) : P;
-        out.put16(o + x, uv, m);
+    out.put16(o, v, m0);
+    for (uint64_t k = 16; k < n; k += 16) {
+        const uint32_t m = n - k < 16 ? static_cast<uint32_t>(n - k) : 16u;
+        out.put16(o + k, out.fetch16(o + k - d, m), m);
     }
 }
 
