@@ -50,7 +50,7 @@ constexpr uint32_t kRelStop = 0xffffu;       // packed-step marker: take the gen
 constexpr uint32_t kRefill = 512;            // input progress between window refills
 constexpr uint32_t kWarpSmem = kRing + kIn;
 constexpr unsigned kFull = 0xffffffffu;
-static_assert(kBatchMax + 20 <= kRing, "a batch never overwrites unflushed bytes");
+static_assert(kBatchMax + 32 <= kRing, "a batch never overwrites unflushed bytes");
 
 // Per-launch (or per size bucket) shape of the decode: parse reach (input
 // bytes past a group's first token that must have landed in the window
@@ -477,18 +477,13 @@ struct Out {
     __device__ __forceinline__ void put16(uint64_t x, const uint4& v, uint32_t m) const {
         const uint32_t ix = idx(x);
         const uint32_t sb = ix & 3, sh = 8 * sb;
-        uint64_t lo = (static_cast<uint64_t>(v.y) << 32) | v.x;
-        uint64_t hi = (static_cast<uint64_t>(v.w) << 32) | v.z;
-        if (m < 16) {
-            if (m <= 8) {
-                hi = 0;
-                if (m < 8) lo &= (1ull << (8 * m)) - 1;
-            } else {
-                hi &= (1ull << (8 * (m - 8))) - 1;
-            }
-        }
-        const uint32_t w0 = static_cast<uint32_t>(lo), w1 = static_cast<uint32_t>(lo >> 32);
-        const uint32_t w2 = static_cast<uint32_t>(hi), w3 = static_cast<uint32_t>(hi >> 32);
+        // keep bytes [0, m): word j keeps its low 8 m - 32 j bits (0..32),
+        // a right funnel shift of ones by the rest (clamped at 32)
+        const uint32_t bits = 8 * m;
+        const uint32_t w0 = v.x & __funnelshift_rc(~0u, 0u, bits >= 32 ? 0u : 32u - bits);
+        const uint32_t w1 = v.y & __funnelshift_rc(~0u, 0u, bits >= 64 ? 0u : 64u - bits);
+        const uint32_t w2 = v.z & __funnelshift_rc(~0u, 0u, bits >= 96 ? 0u : 96u - bits);
+        const uint32_t w3 = v.w & __funnelshift_rc(~0u, 0u, 128u - bits);
         const uint32_t last = (sb + m - 1) >> 2;  // last word touched, 0..4
         uint32_t* r32 = reinterpret_cast<uint32_t*>(ring);
         constexpr uint32_t kMask = kRing / 4 - 1;
@@ -500,21 +495,24 @@ struct Out {
         if (last >= 4) atomicOr(r32 + ((wi + 4) & kMask), __funnelshift_l(w3, 0u, sh));
     }
 
-    // Zero the ring bytes of output positions [b, e) (e - b <= kRing - 16)
-    // before a batch ORs its bytes in; bytes below b in the first word keep
-    // their contents, up to 3 bytes past e may be cleared too (they belong
-    // to later output, whose batch clears them again). The caller keeps vlo
-    // above every position whose slot this clears.
+    // Zero the ring bytes of output positions [b, e) (e - b <= kRing - 32)
+    // before a batch ORs its bytes in. Bytes below b in the first word keep
+    // their contents; the rest of that word's 16-byte block is cleared word
+    // by word, then whole 16-byte blocks through the one holding e - 1, so
+    // up to 15 bytes past e may be cleared too (they belong to later output,
+    // whose batch clears them again). The caller keeps vlo above every
+    // position whose slot this clears.
     __device__ __forceinline__ void clear(uint64_t b, uint64_t e, uint32_t lane) const {
         if (e <= b) return;
         uint32_t* r32 = reinterpret_cast<uint32_t*>(ring);
-        constexpr uint32_t kMask = kRing / 4 - 1;
         const uint32_t ib = idx(b);
         const uint32_t sb = ib & 3;
         const uint32_t w0 = ib >> 2;
         if (lane == 0) atomicAnd(r32 + w0, (1u << (8 * sb)) - 1);
-        const uint32_t nw = static_cast<uint32_t>((e - b + sb + 3) >> 2);  // words from w0
-        for (uint32_t k = 1 + lane; k < nw; k += 32) r32[(w0 + k) & kMask] = 0;
+        if (lane >= 1 && lane < 4 - (w0 & 3)) r32[w0 + lane] = 0;  // same block: no wrap
+        const uint32_t end = ib + static_cast<uint32_t>(e - b);     // unwrapped ring index
+        for (uint32_t x = (ib & ~15u) + 16 + 16 * lane; x < end; x += 512)
+            *reinterpret_cast<uint4*>(ring + (x & (kRing - 1))) = make_uint4(0, 0, 0, 0);
         __syncwarp();
     }
 
@@ -547,11 +545,16 @@ struct Out {
 // are there.
 __device__ __forceinline__ uint4 in16(const In& in, uint64_t a, uint32_t m) {
     if (in.held(a, m)) {
+        // the five aligned window words the 16 bytes touch, joined by
+        // funnel shifts
+        constexpr uint32_t kMask = kIn / 4 - 1;
         const uint32_t ia = static_cast<uint32_t>((in.gbase + a) & (kIn - 1));
-        const uint32_t b0 = ia & ~15u, b1 = (b0 + 16) & (kIn - 1);
-        const uint4 lo = *reinterpret_cast<const uint4*>(in.win + b0);
-        const uint4 hi = *reinterpret_cast<const uint4*>(in.win + b1);
-        return shift32(lo, hi, ia & 15);
+        const uint32_t wi = ia >> 2, sh = (ia & 3) * 8;
+        const uint32_t* w32 = reinterpret_cast<const uint32_t*>(in.win);
+        const uint32_t w0 = w32[wi], w1 = w32[(wi + 1) & kMask], w2 = w32[(wi + 2) & kMask];
+        const uint32_t w3 = w32[(wi + 3) & kMask], w4 = w32[(wi + 4) & kMask];
+        return make_uint4(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh),
+                          __funnelshift_r(w2, w3, sh), __funnelshift_r(w3, w4, sh));
     }
     return ld16_input(in.g + a, m);
 }
@@ -825,9 +828,9 @@ __device__ __forceinline__ void exec_small(Out& out, const In& in, bool act, uin
                                            uint64_t li, uint64_t lsrc, uint64_t mi,
                                            uint32_t off, uint64_t bstart, uint64_t bend,
                                            uint32_t first, uint32_t lane) {
-    // clear() may zero up to 3 bytes past bend, whose slots held positions
-    // up to bend + 3 - kRing: those are read back from the destination.
-    if (bend + 4 > out.vlo + kRing) out.vlo = bend + 4 - kRing;
+    // clear() may zero up to 15 bytes past bend, whose slots held positions
+    // up to bend + 15 - kRing: those are read back from the destination.
+    if (bend + 16 > out.vlo + kRing) out.vlo = bend + 16 - kRing;
     out.clear(bstart, bend, lane);
     const uint64_t ms = o + li;
     if (act && li) copy_literal(out, in, lsrc, o, li);
