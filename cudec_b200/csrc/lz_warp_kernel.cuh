@@ -426,6 +426,20 @@ __device__ __forceinline__ uint4 ld16_output(const uint8_t* p, uint32_t m) {
     return shift32(lo, hi, mis);
 }
 
+// m (1..16) output bytes at p, read as the aligned words that hold them
+// (no word past the last wanted byte is touched) joined by funnel shifts.
+__device__ __forceinline__ uint4 ld16_words(const uint8_t* p, uint32_t m) {
+    const uintptr_t ad = reinterpret_cast<uintptr_t>(p);
+    const uint32_t s4 = static_cast<uint32_t>(ad & 3), sh = 8 * s4;
+    const uint32_t* q = reinterpret_cast<const uint32_t*>(ad - s4);
+    const uint32_t lw = (s4 + m - 1) >> 2;  // last word holding a wanted byte, 0..4
+    const uint32_t w0 = q[0];
+    const uint32_t w1 = lw >= 1 ? q[1] : 0u, w2 = lw >= 2 ? q[2] : 0u;
+    const uint32_t w3 = lw >= 3 ? q[3] : 0u, w4 = lw >= 4 ? q[4] : 0u;
+    return make_uint4(__funnelshift_r(w0, w1, sh), __funnelshift_r(w1, w2, sh),
+                      __funnelshift_r(w2, w3, sh), __funnelshift_r(w3, w4, sh));
+}
+
 // Per-warp output state. Positions are byte offsets into the chunk's output.
 struct Out {
     uint8_t* ring;     // kRing bytes of shared memory
@@ -457,7 +471,7 @@ struct Out {
     // when a source may straddle vlo with its upper bytes in the ring alone.
     __device__ __forceinline__ uint4 fetch16(uint64_t a, uint32_t m) const {
         if (a >= vlo) return ring16(a);
-        if (a + m <= flushed) return ld16_output(dst + a, m);
+        if (a + m <= flushed) return ld16_words(dst + a, m);
         uint32_t w[4] = {0, 0, 0, 0};
 #pragma unroll
         for (uint32_t j = 0; j < 16; ++j) {
@@ -472,8 +486,8 @@ struct Out {
 
     // Write the first m (1..16) bytes of v at output position x (ring). The
     // ring bytes of the current batch start at zero (clear()) and every byte
-    // has one writer, so the bytes are OR-ed in as (at most five) aligned
-    // words; neighbouring lanes may share the edge words.
+    // has one writer, so the bytes are OR-ed in as five aligned words;
+    // neighbouring lanes may share the edge words.
     __device__ __forceinline__ void put16(uint64_t x, const uint4& v, uint32_t m) const {
         const uint32_t ix = idx(x);
         const uint32_t sb = ix & 3, sh = 8 * sb;
@@ -484,15 +498,16 @@ struct Out {
         const uint32_t w1 = v.y & __funnelshift_rc(~0u, 0u, bits >= 64 ? 0u : 64u - bits);
         const uint32_t w2 = v.z & __funnelshift_rc(~0u, 0u, bits >= 96 ? 0u : 96u - bits);
         const uint32_t w3 = v.w & __funnelshift_rc(~0u, 0u, 128u - bits);
-        const uint32_t last = (sb + m - 1) >> 2;  // last word touched, 0..4
+        // all five words: past the last byte they are zero, and OR-ing zero
+        // leaves a word as it is
         uint32_t* r32 = reinterpret_cast<uint32_t*>(ring);
         constexpr uint32_t kMask = kRing / 4 - 1;
         const uint32_t wi = ix >> 2;
         atomicOr(r32 + wi, w0 << sh);
-        if (last >= 1) atomicOr(r32 + ((wi + 1) & kMask), __funnelshift_l(w0, w1, sh));
-        if (last >= 2) atomicOr(r32 + ((wi + 2) & kMask), __funnelshift_l(w1, w2, sh));
-        if (last >= 3) atomicOr(r32 + ((wi + 3) & kMask), __funnelshift_l(w2, w3, sh));
-        if (last >= 4) atomicOr(r32 + ((wi + 4) & kMask), __funnelshift_l(w3, 0u, sh));
+        atomicOr(r32 + ((wi + 1) & kMask), __funnelshift_l(w0, w1, sh));
+        atomicOr(r32 + ((wi + 2) & kMask), __funnelshift_l(w1, w2, sh));
+        atomicOr(r32 + ((wi + 3) & kMask), __funnelshift_l(w2, w3, sh));
+        atomicOr(r32 + ((wi + 4) & kMask), __funnelshift_l(w3, 0u, sh));
     }
 
     // Zero the ring bytes of output positions [b, e) (e - b <= kRing - 32)
