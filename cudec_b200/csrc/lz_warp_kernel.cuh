@@ -576,55 +576,53 @@ __device__ __forceinline__ uint4 in16(const In& in, uint64_t a, uint32_t m) {
 
 // Copy n input bytes from position src to output position o.
 __device__ __forceinline__ void copy_literal(const Out& out, const In& in, uint64_t src,
-                                             uint64_t o, uint64_t n) {
-    for (uint64_t k = 0; k < n; k += 16) {
-        const uint32_t m = n - k < 16 ? static_cast<uint32_t>(n - k) : 16u;
+                                             uint64_t o, uint32_t n) {
+    for (uint32_t k = 0; k < n; k += 16) {
+        const uint32_t m = n - k < 16 ? n - k : 16u;
         out.put16(o + k, in16(in, src + k, m), m);
     }
 }
 
 // Output [o, o + n) = the match with offset off (out[x] = out[x - off]);
 // every source byte below o is already written.
-__device__ __forceinline__ void copy_match(const Out& out, uint64_t o, uint64_t n, uint32_t off) {
+__device__ __forceinline__ void copy_match(const Out& out, uint64_t o, uint32_t n, uint32_t off) {
     // The first piece is one fetch and one write in every lane. With a
     // period off < 16 the fetch holds the period alone; it is expanded to 16
-    // bytes in registers by doubling (a prefix of length off * 2^k repeated
-    // next to itself keeps period off), and every later byte repeats the one
+    // bytes in registers, and every later byte repeats the one
     // Q = off * ceil(16 / off) (16..30) bytes back, which is written by then:
     // the rest of the match is the plain copy at distance Q.
-    const uint32_t m0 = n < 16 ? static_cast<uint32_t>(n) : 16u;
+    const uint32_t m0 = n < 16 ? n : 16u;
     uint4 v = out.fetch16(o - off, off < 16 ? off : m0);
-    uint32_t d = off;
-    if (off < 16) {
+    {
         const uint64_t lo = (static_cast<uint64_t>(v.y) << 32) | v.x;
         const uint64_t hi = (static_cast<uint64_t>(v.w) << 32) | v.z;
-        uint64_t olo, ohi;
-        if (off <= 8) {
-            // the period in the low off bytes, doubled to 8 bytes; the next 8
-            // bytes start r = 8 mod off bytes into the period: byte j of them
-            // is byte j + r of the first 8 (j < 8 - r) or byte j + r - off
-            const uint32_t s = 8 * off;  // 8..64
-            olo = lo & (~0ull >> (64 - s));
-            olo |= s < 64 ? olo << (s & 63) : 0ull;
-            olo |= s < 32 ? olo << ((2 * s) & 63) : 0ull;
-            olo |= s < 16 ? olo << ((4 * s) & 63) : 0ull;
-            // 8 mod off for off = 1..8, one nibble each
-            const uint32_t r = static_cast<uint32_t>((0x012302000ull >> (4 * off)) & 15);
-            ohi = (olo >> (8 * r)) | (olo << ((8 * (off - r)) & 63));
-        } else {
-            // 9..15 bytes: the first 16 - off of them repeat once
-            const uint32_t s = 8 * (off - 8);  // 8..56
-            olo = lo;
-            ohi = (hi & ((1ull << s) - 1)) | (lo << s);
-        }
-        v = make_uint4(static_cast<uint32_t>(olo), static_cast<uint32_t>(olo >> 32),
-                       static_cast<uint32_t>(ohi), static_cast<uint32_t>(ohi >> 32));
-        // Q - 16 for off = 1..15, one nibble each
-        d = 16 + static_cast<uint32_t>((0xECA8642052402000ull >> (4 * off)) & 15);
+        // off <= 8: the period in the low off bytes, doubled to 8 bytes; the
+        // next 8 bytes start r = 8 mod off bytes into the period, so byte j
+        // of them is byte j + r of the first 8 (j < 8 - r) or byte j + r - off
+        const uint32_t s = 8 * off;  // 8..120
+        uint64_t plo = lo & (~0ull >> ((64 - s) & 63));
+        plo |= s < 64 ? plo << (s & 63) : 0ull;
+        plo |= s < 32 ? plo << ((2 * s) & 63) : 0ull;
+        plo |= s < 16 ? plo << ((4 * s) & 63) : 0ull;
+        // 8 mod off for off = 1..8, one nibble each
+        const uint32_t r = static_cast<uint32_t>((0x012302000ull >> ((4 * off) & 63)) & 15);
+        const uint64_t phi = (plo >> ((8 * r) & 63)) | (plo << ((8 * (off - r)) & 63));
+        // off = 9..15: the first 16 - off bytes repeat once
+        const uint32_t s2 = (s - 64) & 63;  // 8..56
+        const uint64_t qhi = (hi & ((1ull << s2) - 1)) | (lo << s2);
+        const bool small = off <= 8;
+        const uint64_t olo = small ? plo : lo, ohi = small ? phi : qhi;
+        if (off < 16)  // a select: every lane computed the expansion
+            v = make_uint4(static_cast<uint32_t>(olo), static_cast<uint32_t>(olo >> 32),
+                           static_cast<uint32_t>(ohi), static_cast<uint32_t>(ohi >> 32));
     }
+    // Q - 16 for off = 1..15, one nibble each
+    const uint32_t d =
+        off < 16 ? 16 + static_cast<uint32_t>((0xECA8642052402000ull >> (4 * (off & 15))) & 15)
+                 : off;
     out.put16(o, v, m0);
-    for (uint64_t k = 16; k < n; k += 16) {
-        const uint32_t m = n - k < 16 ? static_cast<uint32_t>(n - k) : 16u;
+    for (uint32_t k = 16; k < n; k += 16) {
+        const uint32_t m = n - k < 16 ? n - k : 16u;
         out.put16(o + k, out.fetch16(o + k - d, m), m);
     }
 }
@@ -848,7 +846,7 @@ __device__ __forceinline__ void exec_small(Out& out, const In& in, bool act, uin
     if (bend + 16 > out.vlo + kRing) out.vlo = bend + 16 - kRing;
     out.clear(bstart, bend, lane);
     const uint64_t ms = o + li;
-    if (act && li) copy_literal(out, in, lsrc, o, li);
+    if (act && li) copy_literal(out, in, lsrc, o, static_cast<uint32_t>(li));
     __syncwarp();
     // Matches in rounds: a match copies once no unfinished match's output
     // overlaps the bytes its source reads in this batch ([rs, re), relative
@@ -882,7 +880,7 @@ __device__ __forceinline__ void exec_small(Out& out, const In& in, bool act, uin
         const uint32_t last = cand ? 31 - __clz(cand) : 0u;
         const uint32_t last_end = __shfl_sync(kFull, rme, last);
         const bool ready = pend && (re <= rs || cand == 0 || last_end <= rs);
-        if (ready) copy_match(out, ms, mi, off);
+        if (ready) copy_match(out, ms, static_cast<uint32_t>(mi), off);
         __syncwarp();
         pend = pend && !ready;
         LZW_EV(2, 1);
