@@ -69,7 +69,10 @@ __host__ __device__ constexpr bool tune_valid(const Tune& t) {
 }
 
 // Profiling builds (-DCDB_PHASE_TIMING) accumulate per-phase SM cycles and
-// event counts over all chunks of a launch.
+// event counts over all chunks of a launch. Cycles: 0 window refill, 1 walk,
+// 2 checks, 3 execute (of which 4 clear, 6 literals, 7 match rounds), 5 the
+// whole chunk. Events: 0 groups, 1 tokens, 2 match rounds, 3 tokens copied
+// straight to the destination.
 #ifdef CDB_PHASE_TIMING
 __device__ unsigned long long lzw_cycles[8];
 __device__ unsigned long long lzw_events[8];
@@ -844,10 +847,15 @@ __device__ __forceinline__ void exec_small(Out& out, const In& in, bool act, uin
     // clear() may zero up to 15 bytes past bend, whose slots held positions
     // up to bend + 15 - kRing: those are read back from the destination.
     if (bend + 16 > out.vlo + kRing) out.vlo = bend + 16 - kRing;
+    LZW_T(t_clear);
     out.clear(bstart, bend, lane);
+    LZW_ADD(4, t_clear);
+    LZW_T(t_lit);
     const uint64_t ms = o + li;
     if (act && li) copy_literal(out, in, lsrc, o, static_cast<uint32_t>(li));
     __syncwarp();
+    LZW_ADD(6, t_lit);
+    LZW_T(t_rounds);
     // Matches in rounds: a match copies once no unfinished match's output
     // overlaps the bytes its source reads in this batch ([rs, re), relative
     // to bstart; everything before bstart and every literal is written).
@@ -885,6 +893,7 @@ __device__ __forceinline__ void exec_small(Out& out, const In& in, bool act, uin
         pend = pend && !ready;
         LZW_EV(2, 1);
     }
+    LZW_ADD(7, t_rounds);
     out.flush(bend, false, lane);
 }
 
