@@ -214,49 +214,22 @@ __device__ __forceinline__ int first_event(bool err, int st, uint32_t refill_ev,
     return CUDEC_ERR_CORRUPT_INPUT;
 }
 
-// Copy [o, o + n) from o - d inside the page's output (d <= o), one lane:
-// 16-byte windows (two aligned loads and a funnel shift, then the widest
-// stores the destination's alignment allows); a period d < 16 is expanded
-// to 16 bytes by doubling (a prefix of length d * 2^k next to itself keeps
-// period d) and written every P bytes, P the largest multiple of d up to 16.
-// Every byte a window reads was written before it, by this lane or earlier.
+// Copy [o, o + n) from o - d inside the page's output (d <= o), one lane,
+// in 16-byte windows: the aligned words holding the bytes, joined by funnel
+// shifts, then the widest stores the destination's alignment allows. The
+// first window is one read and one write in every lane (a distance under 16
+// is expanded to 16 bytes by lzw::period16), the rest a plain copy at
+// lzw::rest_distance(d). Every byte a window reads was written before it, by
+// this lane or earlier.
 __device__ __forceinline__ void page_copy(uint8_t* out, uint32_t o, uint32_t n, uint32_t d) {
     uint8_t* D = out + o;
-    if (d >= 16) {
-        for (uint32_t k = 0; k < n; k += 16) {
-            const uint32_t m = n - k < 16 ? n - k : 16u;
-            lzw::st16_global(D + k, lzw::ld16_output(D + k - d, m), m);
-        }
-        return;
+    const uint32_t m0 = n < 16 ? n : 16u;
+    lzw::st16_global(D, lzw::period16(lzw::ld16_words(D - d, d < 16 ? d : m0), d), m0);
+    const uint32_t q = lzw::rest_distance(d);
+    for (uint32_t k = 16; k < n; k += 16) {
+        const uint32_t m = n - k < 16 ? n - k : 16u;
+        lzw::st16_global(D + k, lzw::ld16_words(D + k - q, m), m);
     }
-    const uint4 v = lzw::ld16_output(D - d, d);
-    uint64_t lo = (static_cast<uint64_t>(v.y) << 32) | v.x;
-    uint64_t hi = (static_cast<uint64_t>(v.w) << 32) | v.z;
-    if (d < 8) {
-        lo &= (1ull << (8 * d)) - 1;
-        hi = 0;
-    } else if (d > 8) {
-        hi &= (1ull << (8 * (d - 8))) - 1;
-    } else {
-        hi = 0;
-    }
-#pragma unroll
-    for (uint32_t len = d, k = 0; k < 4; ++k, len <<= 1) {
-        if (len < 16) {
-            if (len < 8) {
-                hi |= (hi << (8 * len)) | (lo >> (64 - 8 * len));
-                lo |= lo << (8 * len);
-            } else {
-                hi |= lo << (8 * (len - 8));
-            }
-        }
-    }
-    const uint4 uv = make_uint4(static_cast<uint32_t>(lo), static_cast<uint32_t>(lo >> 32),
-                                static_cast<uint32_t>(hi), static_cast<uint32_t>(hi >> 32));
-    // P - 1 for d = 1..15, one nibble each
-    const uint32_t P = static_cast<uint32_t>((0xEDCBA98FDBEFEFF0ull >> (4 * d)) & 15) + 1;
-    for (uint32_t x = 0; x < n; x += P)
-        lzw::st16_global(D + x, uv, n - x < P ? n - x : P);
 }
 
 // Decode one page; every lane returns the same status and *written. Output

@@ -588,42 +588,50 @@ __device__ __forceinline__ void copy_literal(const Out& out, const In& in, uint6
 
 // Output [o, o + n) = the match with offset off (out[x] = out[x - off]);
 // every source byte below o is already written.
-__device__ __forceinline__ void copy_match(const Out& out, uint64_t o, uint32_t n, uint32_t off) {
-    // The first piece is one fetch and one write in every lane. With a
-    // period off < 16 the fetch holds the period alone; it is expanded to 16
-    // bytes in registers, and every later byte repeats the one
-    // Q = off * ceil(16 / off) (16..30) bytes back, which is written by then:
-    // the rest of the match is the plain copy at distance Q.
-    const uint32_t m0 = n < 16 ? n : 16u;
-    uint4 v = out.fetch16(o - off, off < 16 ? off : m0);
-    {
-        const uint64_t lo = (static_cast<uint64_t>(v.y) << 32) | v.x;
-        const uint64_t hi = (static_cast<uint64_t>(v.w) << 32) | v.z;
-        // off <= 8: the period in the low off bytes, doubled to 8 bytes; the
-        // next 8 bytes start r = 8 mod off bytes into the period, so byte j
-        // of them is byte j + r of the first 8 (j < 8 - r) or byte j + r - off
-        const uint32_t s = 8 * off;  // 8..120
-        uint64_t plo = lo & (~0ull >> ((64 - s) & 63));
-        plo |= s < 64 ? plo << (s & 63) : 0ull;
-        plo |= s < 32 ? plo << ((2 * s) & 63) : 0ull;
-        plo |= s < 16 ? plo << ((4 * s) & 63) : 0ull;
-        // 8 mod off for off = 1..8, one nibble each
-        const uint32_t r = static_cast<uint32_t>((0x012302000ull >> ((4 * off) & 63)) & 15);
-        const uint64_t phi = (plo >> ((8 * r) & 63)) | (plo << ((8 * (off - r)) & 63));
-        // off = 9..15: the first 16 - off bytes repeat once
-        const uint32_t s2 = (s - 64) & 63;  // 8..56
-        const uint64_t qhi = (hi & ((1ull << s2) - 1)) | (lo << s2);
-        const bool small = off <= 8;
-        const uint64_t olo = small ? plo : lo, ohi = small ? phi : qhi;
-        if (off < 16)  // a select: every lane computed the expansion
-            v = make_uint4(static_cast<uint32_t>(olo), static_cast<uint32_t>(olo >> 32),
-                           static_cast<uint32_t>(ohi), static_cast<uint32_t>(ohi >> 32));
-    }
+// A match at distance off < 16 starts from its period alone: the low off
+// bytes of v. period16 returns the match's first 16 bytes, expanded in
+// registers without branches and computed in every lane. A lane with
+// off >= 16 gets v back. Periods up to 8 bytes are doubled in 64 bits, and
+// the next 8 bytes start r = 8 mod off bytes into the period, so byte j of
+// them is byte j + r of the first 8 (j < 8 - r) or byte j + r - off. For
+// 9..15 bytes, the first 16 - off bytes repeat once. Every later byte of the
+// match repeats the one rest_distance(off) = off * ceil(16 / off) (16..30)
+// bytes back, which is written by then, so the rest of the match is a plain
+// copy at that distance.
+__device__ __forceinline__ uint4 period16(const uint4& v, uint32_t off) {
+    const uint64_t lo = (static_cast<uint64_t>(v.y) << 32) | v.x;
+    const uint64_t hi = (static_cast<uint64_t>(v.w) << 32) | v.z;
+    const uint32_t d = off < 16 ? off : 16u;
+    const uint32_t s = 8 * d;  // 8..128
+    uint64_t plo = lo & (~0ull >> ((64 - s) & 63));
+    plo |= s < 64 ? plo << (s & 63) : 0ull;
+    plo |= s < 32 ? plo << ((2 * s) & 63) : 0ull;
+    plo |= s < 16 ? plo << ((4 * s) & 63) : 0ull;
+    // 8 mod d for d = 1..8, one nibble each
+    const uint32_t r = static_cast<uint32_t>((0x012302000ull >> ((4 * d) & 63)) & 15);
+    const uint64_t phi = (plo >> ((8 * r) & 63)) | (plo << ((8 * (d - r)) & 63));
+    const uint32_t s2 = (s - 64) & 63;
+    const uint64_t qhi = (hi & ((1ull << s2) - 1)) | (lo << s2);
+    const bool small = d <= 8;
+    const uint64_t olo = small ? plo : lo, ohi = small ? phi : qhi;
+    const uint4 e = make_uint4(static_cast<uint32_t>(olo), static_cast<uint32_t>(olo >> 32),
+                               static_cast<uint32_t>(ohi), static_cast<uint32_t>(ohi >> 32));
+    return off < 16 ? e : v;
+}
+
+__device__ __forceinline__ uint32_t rest_distance(uint32_t off) {
     // Q - 16 for off = 1..15, one nibble each
-    const uint32_t d =
-        off < 16 ? 16 + static_cast<uint32_t>((0xECA8642052402000ull >> (4 * (off & 15))) & 15)
-                 : off;
-    out.put16(o, v, m0);
+    return off < 16 ? 16 + static_cast<uint32_t>((0xECA8642052402000ull >> (4 * (off & 15))) & 15)
+                    : off;
+}
+
+// Lane-parallel match copy through the ring: the first piece is one fetch
+// and one write in every lane (period16), the rest a plain copy at
+// rest_distance(off).
+__device__ __forceinline__ void copy_match(const Out& out, uint64_t o, uint32_t n, uint32_t off) {
+    const uint32_t m0 = n < 16 ? n : 16u;
+    out.put16(o, period16(out.fetch16(o - off, off < 16 ? off : m0), off), m0);
+    const uint32_t d = rest_distance(off);
     for (uint32_t k = 16; k < n; k += 16) {
         const uint32_t m = n - k < 16 ? n - k : 16u;
         out.put16(o + k, out.fetch16(o + k - d, m), m);

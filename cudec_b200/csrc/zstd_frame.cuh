@@ -122,7 +122,7 @@ __device__ __forceinline__ void warp_fill(uint8_t* dst, uint8_t b, uint64_t n, u
 __device__ __forceinline__ void lane_copy(uint8_t* dst, const uint8_t* src, uint64_t n) {
     for (uint64_t k = 0; k < n; k += 16) {
         const uint32_t m = n - k < 16 ? static_cast<uint32_t>(n - k) : 16u;
-        lzw::st16_global(dst + k, lzw::ld16_output(src + k, m), m);
+        lzw::st16_global(dst + k, lzw::ld16_words(src + k, m), m);
     }
 }
 
@@ -134,45 +134,18 @@ __device__ __forceinline__ void lane_fill(uint8_t* dst, uint8_t b, uint64_t n) {
 }
 
 // One lane writes the match dst[ms, ms + n) at offset off (every byte before
-// ms is written), 16 bytes at a time. The first piece is one read and one
-// write in every lane: with a period off < 16 the read holds the period
-// alone, expanded to 16 bytes in registers without branches, and every later
-// byte repeats the one Q = off * ceil(16 / off) (16..30) bytes back, which is
-// written by then, so the rest of the match is the plain copy at distance Q.
+// ms is written; off is below the 8 MB window), 16 bytes at a time: the
+// first piece is one read and one write in every lane (lzw::period16 for
+// periods under 16 bytes), the rest a plain copy at lzw::rest_distance(off).
 __device__ __forceinline__ void lane_match(uint8_t* dst, uint64_t ms, uint64_t n, uint64_t off) {
     uint8_t* o = dst + ms;
+    const uint32_t f = static_cast<uint32_t>(off);
     const uint32_t m0 = n < 16 ? static_cast<uint32_t>(n) : 16u;
-    const uint32_t d0 = off < 16 ? static_cast<uint32_t>(off) : 16u;
-    uint4 v = lzw::ld16_words(o - off, off < 16 ? d0 : m0);
-    {
-        const uint64_t lo = (static_cast<uint64_t>(v.y) << 32) | v.x;
-        const uint64_t hi = (static_cast<uint64_t>(v.w) << 32) | v.z;
-        // d0 <= 8: the period in the low d0 bytes, doubled to 8 bytes; the
-        // next 8 bytes start r = 8 mod d0 bytes into the period
-        const uint32_t s = 8 * d0;  // 8..128
-        uint64_t plo = lo & (~0ull >> ((64 - s) & 63));
-        plo |= s < 64 ? plo << (s & 63) : 0ull;
-        plo |= s < 32 ? plo << ((2 * s) & 63) : 0ull;
-        plo |= s < 16 ? plo << ((4 * s) & 63) : 0ull;
-        // 8 mod d for d = 1..8, one nibble each
-        const uint32_t r = static_cast<uint32_t>((0x012302000ull >> ((4 * d0) & 63)) & 15);
-        const uint64_t phi = (plo >> ((8 * r) & 63)) | (plo << ((8 * (d0 - r)) & 63));
-        // d0 = 9..15: the first 16 - d0 bytes repeat once
-        const uint32_t s2 = (s - 64) & 63;
-        const uint64_t qhi = (hi & ((1ull << s2) - 1)) | (lo << s2);
-        const bool small = d0 <= 8;
-        const uint64_t olo = small ? plo : lo, ohi = small ? phi : qhi;
-        if (off < 16)  // a select: every lane computed the expansion
-            v = make_uint4(static_cast<uint32_t>(olo), static_cast<uint32_t>(olo >> 32),
-                           static_cast<uint32_t>(ohi), static_cast<uint32_t>(ohi >> 32));
-    }
-    // Q - 16 for d = 1..15, one nibble each
-    const uint64_t dist =
-        off < 16 ? 16 + ((0xECA8642052402000ull >> (4 * (off & 15))) & 15) : off;
-    lzw::st16_global(o, v, m0);
+    lzw::st16_global(o, lzw::period16(lzw::ld16_words(o - off, f < 16 ? f : m0), f), m0);
+    const uint64_t d = lzw::rest_distance(f);
     for (uint64_t k = 16; k < n; k += 16) {
         const uint32_t m = n - k < 16 ? static_cast<uint32_t>(n - k) : 16u;
-        lzw::st16_global(o + k, lzw::ld16_words(o + k - dist, m), m);
+        lzw::st16_global(o + k, lzw::ld16_words(o + k - d, m), m);
     }
 }
 
