@@ -44,7 +44,7 @@ constexpr uint32_t kInAhead = kIn - 64;      // largest fill distance past the p
 constexpr uint32_t kBatchMax = 4096;         // largest output staged per ring batch
 constexpr uint64_t kBig = 256;               // longer tokens are copied by the whole warp
 constexpr uint32_t kPW = 1024;               // largest parse reach (input bytes landed ahead)
-constexpr uint32_t kHops = 8;                // chain hops per branch in the group walk
+constexpr uint32_t kHops = 4;                // chain hops per branch in the group walk
 constexpr uint32_t kStop = ~0u;              // the group walk stops at this token
 constexpr uint32_t kRelStop = 0xffffu;       // packed-step marker: take the general step
 constexpr uint32_t kRefill = 512;            // input progress between window refills
