@@ -47,7 +47,7 @@ constexpr uint32_t kPW = 1024;               // largest parse reach (input bytes
 constexpr uint32_t kHops = 4;                // chain hops per branch in the group walk
 constexpr uint32_t kStop = ~0u;              // the group walk stops at this token
 constexpr uint32_t kRelStop = 0xffffu;       // packed-step marker: take the general step
-constexpr uint32_t kRefill = 512;            // input progress between window refills
+constexpr uint32_t kRefill = 1024;           // input progress between window refills
 constexpr uint32_t kWarpSmem = kRing + kIn;
 constexpr unsigned kFull = 0xffffffffu;
 static_assert(kBatchMax + 32 <= kRing, "a batch never overwrites unflushed bytes");
