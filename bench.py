@@ -33,7 +33,7 @@ the launch itself is bracketed by CUDA events on its stream.
             graph) against the plain path (one batch launch per format)
   gdeflate  4 GiB as 65,536 pages of 64 KiB in 16,384 TileStreams of
             256 KiB (content: 256-symbol Zipf(1.3) literals, matches 3-258,
-            offsets up to 32 KiB), encoded by this build's GDeflate encoder at
+            offsets up to 32 KiB), encoded by this library's GDeflate encoder at
             its highest effort (dynamic Huffman blocks); `--gdeflate-unique`
             distinct streams are encoded and laid out repeatedly, every page
             its own copy in HBM; one page-batch launch
@@ -386,7 +386,7 @@ def run_gdeflate(torch, cd, DeviceBatch, args, dev, stream, flush, max_over_rank
             "pages": n, "streams": args.gdeflate_streams, "unique_streams": unique,
             "compressed_bytes": in_bytes, "decompressed_bytes": out_bytes,
             "roofline_frac": round((in_bytes + out_bytes) / (ms * 1e-3) / 1e9 / peaks()[0], 5),
-            "encoder": "this build's GDeflate encoder, level 12, 32 KiB window",
+            "encoder": "this library's GDeflate encoder, level 12, 32 KiB window",
             "parity": "vs the build's CPU decoder; GDeflate reference decoder unpinned"}
 
 

@@ -1,8 +1,8 @@
 /* Seeded synthetic content for the benchmark and test workloads.
  *
  * The reference measures on Silesia/enwik8, which are not available here; the
- * workloads are instead BASELINE-shaped synthetic chunks with the same
- * statistics for every run: literal runs (geometric length) over a small
+ * workloads are instead synthetic chunks with the headline configurations'
+ * sizes and the same statistics for every run: literal runs (geometric length) over a small
  * alphabet with Zipf frequencies, alternating with back-references (geometric
  * length, uniform offset), optionally with runs of one repeated byte, or whole
  * chunks of uniform random bytes. Deterministic in (seed, chunk index): the

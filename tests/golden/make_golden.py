@@ -169,7 +169,7 @@ def tilestream_vectors():
 
 
 def gdeflate_vectors():
-    """Pages from this build's own encoder with their decoded digests. No
+    """Pages from this library's own encoder with their decoded digests. No
     GDeflate reference decoder or vector exists in the reference tree, so
     these pin the build's format decisions against later change; they are
     not parity with the GDeflate reference."""
