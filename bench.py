@@ -387,7 +387,7 @@ def run_gdeflate(torch, cd, DeviceBatch, args, dev, stream, flush, max_over_rank
             "compressed_bytes": in_bytes, "decompressed_bytes": out_bytes,
             "roofline_frac": round((in_bytes + out_bytes) / (ms * 1e-3) / 1e9 / peaks()[0], 5),
             "encoder": "this library's GDeflate encoder, level 12, 32 KiB window",
-            "parity": "vs the build's CPU decoder; GDeflate reference decoder unpinned"}
+            "parity": "vs this library's CPU decoder; GDeflate reference decoder unpinned"}
 
 
 SERVE_SEED = 0xC0DEC5

@@ -324,7 +324,7 @@ def _gd():
 
 
 def gdeflate_compress(data, level=12, window=32768):
-    """One GDeflate page (len(data) <= 65536) from the build's own encoder."""
+    """One GDeflate page (len(data) <= 65536) from this library's own encoder."""
     data = bytes(data)
     assert len(data) <= 65536
     cap = 2 * len(data) + 4096

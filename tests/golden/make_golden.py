@@ -171,7 +171,7 @@ def tilestream_vectors():
 def gdeflate_vectors():
     """Pages from this library's own encoder with their decoded digests. No
     GDeflate reference decoder or vector exists in the reference tree, so
-    these pin the build's format decisions against later change; they are
+    these pin this library's format decisions against later change; they are
     not parity with the GDeflate reference."""
     import numpy as np
     out = []

@@ -3,7 +3,7 @@ GPU decoder: its 32-lane refill schedule is trace-identical to the
 reference's src/gdeflate_schedule.h (compiled from the reference's sources)
 on random pages and operation lists; its TileStream walker gives the
 reference walker's verdicts and tile tables on the reference's fuzz seeds
-(tests/golden/tilestream.json) and on mutants; the build's encoder round-trips
+(tests/golden/tilestream.json) and on mutants; this library's encoder round-trips
 through it. Symbol-level parity with the GDeflate reference decoder is
 unpinned: the reference holds no decoder and no page vectors."""
 import hashlib

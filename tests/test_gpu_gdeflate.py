@@ -1,7 +1,7 @@
 """GPU parity for the GDeflate page decoder (cudec_gdeflate_decompress_batch)
 and the TileStream entry: every page's status and bytes equal the oracle's
 (oracle/gdeflate_oracle.c, whose refill schedule and envelope walker are
-pinned to the reference's headers), on the build's golden pages, encoder
+pinned to the reference's headers), on this library's golden pages, encoder
 output across levels, sizes and content (stored, static and dynamic blocks),
 mutants, short capacities and unaligned buffers; nothing past bytes_written
 is touched."""
