@@ -8,7 +8,7 @@
 //
 //   1. the group walk finds the next 32 tokens of the chain: every lane takes
 //      the format's branch-free step at two of the next 64 positions, and
-//      the chain through those positions is followed with shuffles, eight
+//      the chain through those positions is followed with shuffles, four
 //      hops per branch (the uncommon token headers take a general step);
 //      lane k ends up with the k-th token's position and output offset;
 //   2. each lane runs the format's exact accept/reject ladder on its token
@@ -19,11 +19,19 @@
 //      output ring (kRing bytes, indexed by destination address mod kRing,
 //      so ring blocks and destination blocks share alignment): literal runs
 //      first, then matches in rounds (a lane copies once no unfinished
-//      match's output overlaps the bytes its source reads; short periods
-//      are replicated in registers); completed 16-byte blocks leave
-//      the ring as aligned, coalesced 16-byte stores. Match sources older
-//      than the ring are read back from the destination. Longer tokens are
+//      match's output overlaps the bytes its source reads). Every byte has
+//      one writer, so pieces are OR-ed into the cleared ring as five aligned
+//      words; a match's first piece is one fetch and one write in every
+//      lane, a period under 16 bytes expanded in registers (period16), the
+//      rest copied at rest_distance. Completed 16-byte blocks leave the
+//      ring as aligned, coalesced 16-byte stores. Match sources older than
+//      the ring are read back from the destination. Longer tokens are
 //      copied by the whole warp straight to the destination.
+//
+// On this in-order, latency-bound warp a data-dependent branch that splits
+// the lanes costs more than the work it skips, so the copy paths compute
+// and select (masks by clamped funnel shifts, all five OR-words, the period
+// expansion in every lane) rather than branch per lane.
 //
 // Statuses follow the reference ladders exactly: LZ4 iderex/cudec
 // src/lz4_block.h:95-258, Snappy src/snappy_block.h:172-435.
