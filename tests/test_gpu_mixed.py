@@ -132,3 +132,47 @@ def test_tuner_keeps_results_and_reports_valid_shapes(cuda):
     torch.cuda.synchronize()
     check(b, recs, outs, "tuned")
     plan.close()
+
+
+def test_edge_cases_in_one_mixed_batch(cuda):
+    """The per-format edge cases in one persistent launch: LZ4 and Snappy
+    matches reading back across a token copied straight to the destination,
+    Zstd frames outside the subset next to one that decodes, and GDeflate
+    pages whose codes pass the 10-bit lookup table. Records and bytes equal
+    each format's own entry and the oracle."""
+    import torch
+    from cudec_b200.device import DeviceBatch
+    from lz_blocks import lz4_block, snappy_block, straddle_blocks
+    import zstd_subset
+    comps, caps, fmts = [], [], []
+    for fmt, make in (("lz4", lz4_block), ("snappy", snappy_block)):
+        for seqs, tail in straddle_blocks(23):
+            c = make(seqs, tail)
+            comps.append(c)
+            caps.append(len(ORACLE[fmt](c, 1 << 16)[1]))
+            fmts.append(fmt)
+    for frame, cap, _ in zstd_subset.refused_frames().values():
+        comps.append(frame)
+        caps.append(cap)
+        fmts.append("zstd")
+    comps.append(W.zstd_compress(zstd_subset.RAW, 3))
+    caps.append(len(zstd_subset.RAW))
+    fmts.append("zstd")
+    rng = np.random.default_rng(5)
+    for ratio in (0.6, 0.85):
+        w = ratio ** np.arange(256)
+        raw = rng.choice(256, size=65536, p=w / w.sum()).astype(np.uint8).tobytes()
+        comps.append(W.gdeflate_compress(raw, 12))
+        caps.append(len(raw))
+        fmts.append("gdeflate")
+    recs, outs = per_format(cuda, comps, caps, fmts)
+    for i in range(len(comps)):
+        st, out = ORACLE[fmts[i]](comps[i], caps[i])
+        assert recs[i] == (st, len(out) if st == 0 else 0), (i, fmts[i], recs[i], st)
+    assert [r[0] for r, f in zip(recs, fmts) if f == "zstd"] == [6, 6, 6, 6, 0]
+    plan = cd.MixedPlan()
+    b = DeviceBatch(comps, caps, device=cuda)
+    assert b.run_mixed(plan, fmts) == 0
+    torch.cuda.synchronize()
+    check(b, recs, outs, "edge cases")
+    plan.close()
