@@ -54,7 +54,7 @@ constexpr uint64_t kBig = 256;               // longer tokens are copied by the 
 constexpr uint32_t kPW = 1024;               // largest parse reach (input bytes landed ahead)
 constexpr uint32_t kHops = 4;                // chain hops per branch in the group walk
 constexpr uint32_t kStop = ~0u;              // the group walk stops at this token
-constexpr uint32_t kRelStop = 0xffffu;       // packed-step marker: take the general step
+constexpr uint32_t kWordStop = ~0u;          // packed-step marker: take the general step
 constexpr uint32_t kRefill = 1024;           // input progress between window refills
 constexpr uint32_t kWarpSmem = kRing + kIn;
 constexpr unsigned kFull = 0xffffffffu;
@@ -730,28 +730,34 @@ __device__ __noinline__ Walk walk_group(const uint8_t* win, uint32_t gb, uint32_
         uint32_t n0, l0, n1, l1;
         const bool k0 = F::step_simple(win, gb, e, r + lane, &n0, &l0);
         const bool k1 = F::step_simple(win, gb, e, r + 32 + lane, &n1, &l1);
-        // packed per position: next token relative to r (below 512, or
-        // kRelStop) | output length << 16 (below 2^10)
-        const uint32_t pk0 = k0 ? (n0 - r) | (l0 << 16) : kRelStop;
-        const uint32_t pk1 = k1 ? (n1 - r) | (l1 << 16) : kRelStop;
-        uint32_t cur = 0;
+        // packed per position: next token relative to r (below 512) |
+        // output length << 16 (below 2^10), or kWordStop for the general step
+        const uint32_t pk0 = k0 ? (n0 - r) | (l0 << 16) : kWordStop;
+        const uint32_t pk1 = k1 ? (n1 - r) | (l1 << 16) : kWordStop;
+        uint32_t cur = 0, prev = 0;
         bool alive = true;
         while (alive) {
 #pragma unroll
             for (uint32_t u = 0; u < kHops; ++u) {
-                // cur is the same in every lane: each lane offers the half
-                // of the 64 positions cur lies in, and one shuffle reads it
-                const uint32_t pk = __shfl_sync(kFull, cur < 32 ? pk0 : pk1, cur & 31);
-                const uint32_t nx = pk & 0xffffu, ln = pk >> 16;
-                const bool take = alive & (nx != kRelStop);
+                // The previous token's word is the next shuffle's index (the
+                // source lane is taken modulo 32, and the word's low bits are
+                // the next position); both halves are read and bit 5 picks
+                // one, so a hop's dependent path is one shuffle and a select.
+                // After the chain stops, the reads are masked by alive.
+                const uint32_t a = __shfl_sync(kFull, pk0, prev);
+                const uint32_t b = __shfl_sync(kFull, pk1, prev);
+                const uint32_t pk = (prev & 32) ? b : a;
+                const bool take = alive & (pk != kWordStop);
                 if (take & (lane == cnt)) {
                     myr = r + cur;
                     myo = od;
                 }
+                const uint32_t nx = pk & 0xffffu;
                 cnt += take ? 1u : 0u;
-                od += take ? ln : 0u;
+                od += take ? pk >> 16 : 0u;
                 alive = take & (cnt < 32) & (nx < 64);
                 cur = take ? nx : cur;
+                prev = pk;
             }
         }
         r += cur;
