@@ -57,6 +57,7 @@ def oracle_lib():
         "oracle_lz4f_decode": (ctypes.c_int, _DEC),
         "oracle_zstd_decode": (ctypes.c_int, _DEC),
         "oracle_xxh64": (ctypes.c_uint64, [_U8P, _U64, _U64]),
+        "oracle_xxh32": (ctypes.c_uint32, [_U8P, _U64, ctypes.c_uint32]),
         "oracle_lz4_decode_batch": (ctypes.c_int, _BATCH),
         "oracle_snappy_decode_batch": (ctypes.c_int, _BATCH),
         "codec_decode_batch": (ctypes.c_int, [ctypes.c_int] + _BATCH),
@@ -106,6 +107,18 @@ def _decode_one(fn, comp, cap):
     w = _U64(0)
     st = fn(src.ctypes.data, len(comp), out.ctypes.data, cap, ctypes.byref(w))
     return st, (out[:w.value].tobytes() if st == 0 else b"")
+
+
+def xxh32(data, seed=0):
+    """XXH32 from the C restatement (LZ4 frame header/block/content checks)."""
+    b = np.frombuffer(bytes(data) or b"\0", dtype=np.uint8)
+    return int(oracle_lib().oracle_xxh32(b.ctypes.data, len(data), seed))
+
+
+def xxh64(data, seed=0):
+    """XXH64 from the C restatement (Zstd content checksum)."""
+    b = np.frombuffer(bytes(data) or b"\0", dtype=np.uint8)
+    return int(oracle_lib().oracle_xxh64(b.ctypes.data, len(data), seed))
 
 
 def lz4_decode(comp, cap):
