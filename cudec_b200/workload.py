@@ -180,6 +180,47 @@ def lz4f_compress(data, block_size_id=4, independent=True, content_checksum=Fals
     return out.raw[:n]
 
 
+
+def lz4f_decompress_ref(frame, cap):
+    """liblz4's frame decoder (LZ4F_decompress, checksums verified): the
+    bytes of the first frame when it decodes within cap bytes, else None.
+    Bytes after the frame are left unread, as the reference's frame entry
+    leaves them (src/frame.cpp:340-397 stops at the end mark and the content
+    checksum)."""
+    L = _lz4lib()
+    L.LZ4F_createDecompressionContext.restype = ctypes.c_size_t
+    L.LZ4F_createDecompressionContext.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_uint]
+    L.LZ4F_freeDecompressionContext.restype = ctypes.c_size_t
+    L.LZ4F_freeDecompressionContext.argtypes = [ctypes.c_void_p]
+    L.LZ4F_decompress.restype = ctypes.c_size_t
+    L.LZ4F_decompress.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t),
+                                  ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t),
+                                  ctypes.c_void_p]
+    L.LZ4F_isError.restype = ctypes.c_uint
+    L.LZ4F_isError.argtypes = [ctypes.c_size_t]
+    dctx = ctypes.c_void_p()
+    if L.LZ4F_isError(L.LZ4F_createDecompressionContext(ctypes.byref(dctx), 100)):
+        raise RuntimeError("LZ4F_createDecompressionContext failed")
+    try:
+        src = ctypes.create_string_buffer(bytes(frame), max(len(frame), 1))
+        out = ctypes.create_string_buffer(max(cap, 1))
+        sp = dp = 0
+        while True:
+            ssz = ctypes.c_size_t(len(frame) - sp)
+            dsz = ctypes.c_size_t(cap - dp)
+            r = L.LZ4F_decompress(dctx, ctypes.byref(out, dp), ctypes.byref(dsz),
+                                  ctypes.byref(src, sp), ctypes.byref(ssz), None)
+            if L.LZ4F_isError(r):
+                return None
+            sp += ssz.value
+            dp += dsz.value
+            if r == 0:
+                return out.raw[:dp]
+            if ssz.value == 0 and dsz.value == 0:
+                return None  # needs input that is not there, or room that is not there
+    finally:
+        L.LZ4F_freeDecompressionContext(dctx)
+
 _zstd = None
 
 
