@@ -34,9 +34,8 @@ the launch itself is bracketed by CUDA events on its stream.
   gdeflate  4 GiB as 65,536 pages of 64 KiB in 16,384 TileStreams of
             256 KiB (content: 256-symbol Zipf(1.3) literals, matches 3-258,
             offsets up to 32 KiB), encoded by this library's GDeflate encoder at
-            its highest effort (dynamic Huffman blocks); `--gdeflate-unique`
-            distinct streams are encoded and laid out repeatedly, every page
-            its own copy in HBM; one page-batch launch
+            its highest effort (dynamic Huffman blocks), every stream distinct;
+            one page-batch launch
   serve     the served mixed-format stream: Poisson arrivals, each request
             1-4,096 chunks (log-uniform), 40 % LZ4 / 20 % Snappy / 30 % Zstd
             level 3 / 10 % GDeflate (one page each, so capped at 64 KiB),
@@ -48,9 +47,14 @@ the launch itself is bracketed by CUDA events on its stream.
   per_format    the same measurement for raw Snappy (same content) and for
             Zstd: 4,096 frames of 1 MiB (1 MiB window, 128 KiB blocks, 10%
             repeated-byte runs, back-references up to 1 MiB), libzstd level 3
-            and level 19 as two batches; `--zstd-unique` distinct frames are
-            compressed and laid out repeatedly so the batch fills 4 GiB of
-            output (every frame is its own copy in HBM; L2 flushed)
+            and level 19 as two batches, every frame distinct (4 GiB of output
+            per batch; L2 flushed)
+  reference_gpu the reference library's own sm_100a LZ4 kernel on the same
+            device batch, flush and events (a baseline leg)
+
+Every leg checks every chunk: statuses and lengths, and the decoded bytes
+against the generator's bytes (or their BLAKE2b digests, taken when the
+input was generated); each leg reports `verified_chunks`.
 
 `--impl reference` times that reference CPU decoder alone, same metric.
 Multi-GPU: replicas (chunks are independent; no exchange step).
@@ -95,16 +99,24 @@ def parse_args():
                     help="Poisson arrival rate of the served stream (requests/s)")
     ap.add_argument("--gdeflate-streams", type=int, default=16384,
                     help="256 KiB TileStreams of the GDeflate leg (0 skips it)")
-    ap.add_argument("--gdeflate-unique", type=int, default=512,
-                    help="distinct TileStreams encoded for the GDeflate leg")
+    ap.add_argument("--gdeflate-unique", type=int, default=0,
+                    help="distinct TileStreams encoded for the GDeflate leg (0: all "
+                         "of them; a smaller count is laid out repeatedly)")
     ap.add_argument("--zstd-frames", type=int, default=4096,
                     help="Zstd frames per batch (0 skips the Zstd legs)")
-    ap.add_argument("--zstd-unique", type=int, default=128,
-                    help="distinct Zstd frames compressed per level")
+    ap.add_argument("--zstd-unique", type=int, default=0,
+                    help="distinct Zstd frames compressed per level (0: all of them; "
+                         "a smaller count is laid out repeatedly)")
     return ap.parse_args()
 
 
 ZSTD_FRAME = 1 << 20
+
+
+def digest(b):
+    """16-byte BLAKE2b digest of a chunk's expected (or decoded) bytes."""
+    import hashlib
+    return hashlib.blake2b(b, digest_size=16).digest()
 
 
 def _zstd_job(job):
@@ -113,18 +125,65 @@ def _zstd_job(job):
     buf, offs = W.generate([ZSTD_FRAME], [W.zstd_params(0.5, 0.1)],
                            seeds=np.array([seed], dtype=np.uint64))
     raw = buf[:ZSTD_FRAME].tobytes()
-    return raw, W.zstd_compress(raw, level, 20, False)
+    return digest(raw), W.zstd_compress(raw, level, 20, False)
 
 
-def zstd_workload(unique, level):
-    """`unique` distinct 1 MiB frames at `level`, compressed in worker
-    processes (spawned, so no CUDA state is forked)."""
+def start_generation(args):
+    """Compress the Zstd frames (both levels) and encode the GDeflate
+    TileStreams in spawned worker processes (no CUDA state is forked), all
+    host cores, while the device legs run. Returns {name: AsyncResult}."""
     import multiprocessing as mp
     from cudec_b200 import workload as W
-    jobs = [(W.chunk_seed(CONFIG_SEED, 3, i), level) for i in range(unique)]
-    with mp.get_context("spawn").Pool(min(os.cpu_count() or 1, 32)) as pool:
-        out = pool.map(_zstd_job, jobs)
-    return [o[0] for o in out], [o[1] for o in out]
+    jobs = {}
+    if args.zstd_frames <= 0 and args.gdeflate_streams <= 0:
+        return None, jobs
+    pool = mp.get_context("spawn").Pool(min(os.cpu_count() or 1, 64))
+    if args.gdeflate_streams > 0:
+        jobs["gdeflate"] = pool.map_async(
+            _gd_job, range(min(args.gdeflate_unique or args.gdeflate_streams,
+                               args.gdeflate_streams)), chunksize=8)
+    if args.zstd_frames > 0:
+        unique = min(args.zstd_unique or args.zstd_frames, args.zstd_frames)
+        for level in (19, 3):
+            jobs["zstd_l%d" % level] = pool.map_async(
+                _zstd_job, [(W.chunk_seed(CONFIG_SEED, 3, i), level) for i in range(unique)],
+                chunksize=4)
+    pool.close()
+    return pool, jobs
+
+
+def verify_outputs(batch, lengths, expect=None, digests=None, window=256 << 20):
+    """Every chunk's decoded bytes against its expected bytes (`expect[k]`)
+    or digest (`digests[k]`), copied back in windows of whole chunks. Returns
+    the number of chunks verified (all of them, or an AssertionError)."""
+    from concurrent.futures import ThreadPoolExecutor
+    offs = batch.dst_offs
+    n = len(lengths)
+    i = done = 0
+    with ThreadPoolExecutor(max_workers=min(os.cpu_count() or 1, 16)) as ex:
+        while i < n:
+            lo = int(offs[i])
+            j = i + 1
+            while j < n and int(offs[j]) + int(lengths[j]) - lo <= window:
+                j += 1
+            hi = int(offs[j - 1]) + int(lengths[j - 1])
+            host = batch.d_dst[lo:hi].cpu().numpy()
+
+            def check(k):
+                o = int(offs[k]) - lo
+                got = host[o:o + int(lengths[k])]
+                if digests is not None:
+                    return digest(got) == digests[k]
+                e = expect[k]
+                e = np.frombuffer(e, dtype=np.uint8) if isinstance(e, (bytes, bytearray)) else e
+                return np.array_equal(got, e)
+
+            ok = list(ex.map(check, range(i, j), chunksize=256))
+            bad = [k for k, v in zip(range(i, j), ok) if not v]
+            assert not bad, "chunk %d: decoded bytes differ from the expected output" % bad[0]
+            done += j - i
+            i = j
+    return done
 
 
 def workload(n, fmt="lz4"):
@@ -301,14 +360,12 @@ def run_mixed(torch, cd, DeviceBatch, args, dev, stream, flush, max_over_ranks, 
     tuning = plan.tuning()
     res = allb.results()
     assert (res["status"] == 0).all() and (res["bytes_written"] == np.array(caps)).all()
-    for i in range(0, n, max(n // 64, 1)):
-        o = int(allb.dst_offs[i])
-        assert allb.d_dst[o:o + caps[i]].cpu().numpy().tobytes() == raws[i].tobytes()
     steps = max(args.steps // 50, 3)
     p_ms = max_over_ranks(time_region(torch, stream, flush, steps, warm,
                                       lambda: allb.run_mixed(plan, fmts, stream)))
     res = allb.results()
-    assert (res["status"] == 0).all()
+    assert (res["status"] == 0).all() and (res["bytes_written"] == np.array(caps)).all()
+    verified = verify_outputs(allb, caps, expect=raws)
     plan.close()
     del allb
     torch.cuda.empty_cache()
@@ -325,6 +382,8 @@ def run_mixed(torch, cd, DeviceBatch, args, dev, stream, flush, max_over_ranks, 
     q_ms = max_over_ranks(time_region(torch, stream, flush, steps, warm, plain))
     for f, b in subs:
         assert (b.results()["status"] == 0).all()
+        idx = [i for i, x in enumerate(fmts) if x == f]
+        assert verify_outputs(b, [caps[i] for i in idx], expect=[raws[i] for i in idx]) == len(idx)
     del subs
     torch.cuda.empty_cache()
     sizes = np.array(caps)
@@ -333,7 +392,8 @@ def run_mixed(torch, cd, DeviceBatch, args, dev, stream, flush, max_over_ranks, 
         "ms_per_step": round(p_ms, 3),
         "plain_per_format_value": round(world * out_bytes / (q_ms * 1e-3) / 1e9, 3),
         "plain_per_format_ms": round(q_ms, 3),
-        "chunks": n, "decompressed_bytes": out_bytes, "compressed_bytes": in_bytes,
+        "chunks": n, "verified_chunks": verified,
+        "decompressed_bytes": out_bytes, "compressed_bytes": in_bytes,
         "largest_chunk": int(sizes.max()), "median_chunk": int(np.median(sizes)),
         "roofline_frac": round((in_bytes + out_bytes) / (p_ms * 1e-3) / 1e9 / peaks()[0], 5),
         "tuning_per_bucket": [list(t) for t in tuning],
@@ -352,22 +412,22 @@ def _gd_job(i):
                         seeds=np.array([W.chunk_seed(GD_SEED, 3, 4 * i + k) for k in range(4)],
                                        dtype=np.uint64))
     raw = buf.tobytes()
-    return raw, W.gdeflate_tilestream(raw, 12, 32768)
+    return [digest(raw[65536 * k:65536 * (k + 1)]) for k in range(4)], \
+        W.gdeflate_tilestream(raw, 12, 32768)
 
 
-def run_gdeflate(torch, cd, DeviceBatch, args, dev, stream, flush, max_over_ranks, world, warm):
+def run_gdeflate(torch, cd, DeviceBatch, args, dev, stream, flush, max_over_ranks, world, warm,
+                 made):
     """65,536 GDeflate pages (16,384 TileStreams x 4 tiles) in one launch."""
-    import multiprocessing as mp
-    unique = min(args.gdeflate_unique, args.gdeflate_streams)
-    with mp.get_context("spawn").Pool(min(os.cpu_count() or 1, 32)) as pool:
-        made = pool.map(_gd_job, range(unique))
-    pages, raws = [], []
-    for raw, ts in made:
+    unique = len(made)
+    pages, digs = [], []
+    for dg, ts in made:
         st, tiles, total = cd.tilestream_parse(ts, 4)
-        assert st == 0 and total == len(raw)
+        assert st == 0 and total == 4 * 65536
         for k, (off, sz, dsz) in enumerate(tiles):
+            assert dsz == 65536
             pages.append(ts[off:off + sz])
-            raws.append(raw[65536 * k:65536 * k + dsz])
+            digs.append(dg[k])
     n = 4 * args.gdeflate_streams
     comps = [pages[i % len(pages)] for i in range(n)]
     b = DeviceBatch(comps, [65536] * n, device=dev, poison=None)
@@ -375,15 +435,14 @@ def run_gdeflate(torch, cd, DeviceBatch, args, dev, stream, flush, max_over_rank
                                     max(args.steps // 50, 3), warm))
     res = b.results()
     assert (res["status"] == 0).all() and (res["bytes_written"] == 65536).all()
-    for i in range(0, n, max(n // 32, 1)):
-        o = int(b.dst_offs[i])
-        assert b.d_dst[o:o + 65536].cpu().numpy().tobytes() == raws[i % len(raws)]
+    verified = verify_outputs(b, [65536] * n, digests=[digs[i % len(digs)] for i in range(n)])
     out_bytes = 65536 * n
     in_bytes = b.src_bytes
     del b
     torch.cuda.empty_cache()
     return {"value": round(world * out_bytes / (ms * 1e-3) / 1e9, 3), "ms_per_step": round(ms, 3),
             "pages": n, "streams": args.gdeflate_streams, "unique_streams": unique,
+            "verified_chunks": verified,
             "compressed_bytes": in_bytes, "decompressed_bytes": out_bytes,
             "roofline_frac": round((in_bytes + out_bytes) / (ms * 1e-3) / 1e9 / peaks()[0], 5),
             "encoder": "this library's GDeflate encoder, level 12, 32 KiB window",
@@ -414,7 +473,7 @@ def serve_requests(k):
         pinned.numpy()[:] = packed
         reqs.append(dict(packed=pinned.numpy(), pin=pinned, offs=offs, sizes=sizes,
                          caps=[len(r) for r in raws], fmts=fmts,
-                         check=(raws[0].tobytes(), raws[-1].tobytes())))
+                         digests=[digest(r) for r in raws]))
     return reqs
 
 
@@ -441,21 +500,30 @@ def serve_once(cd, reqs, mode, slots, rate):
 
     th = threading.Thread(target=submitter)
     th.start()
-    lats, t_end = [], 0.0
+    lats, t_end, outs = [], 0.0, []
     for i, r in enumerate(reqs):
         while tickets[i] is None:
             time.sleep(0.0002)
         st, recs, ptrs, lat = srv.wait(tickets[i])
         assert st == 0 and (recs["status"] == 0).all()
-        assert read_device(int(ptrs[0]), r["caps"][0]) == r["check"][0]
-        assert read_device(int(ptrs[-1]), r["caps"][-1]) == r["check"][1]
+        assert (recs["bytes_written"] == np.array(r["caps"])).all()
         lats.append(lat)
         t_end = time.perf_counter()
-        srv.release(tickets[i])
+        outs.append(ptrs)
     th.join()
+    # every chunk of every request, read back from the arena after the
+    # replay (outputs stay resident until released; the 32 GiB budget holds
+    # the whole stream, so holding them changes no admission)
+    verified = 0
+    for i, r in enumerate(reqs):
+        for k, cap in enumerate(r["caps"]):
+            assert digest(read_device(int(outs[i][k]), cap)) == r["digests"][k], (i, k)
+            verified += 1
+        srv.release(tickets[i])
     srv.close()
     total = float(sum(sum(r["caps"]) for r in reqs))
-    return {"p50_ms": round(float(np.percentile(lats, 50)), 3),
+    return {"verified_chunks": verified,
+            "p50_ms": round(float(np.percentile(lats, 50)), 3),
             "p99_ms": round(float(np.percentile(lats, 99)), 3),
             "mean_ms": round(float(np.mean(lats)), 3),
             "value": round(total / (t_end - t0) / 1e9, 3),
@@ -475,6 +543,63 @@ def run_serve(cd, args, dev):
             "budget_bytes": 32 << 30, "slots": SERVE_SLOTS,
             "formats": "40 % LZ4 / 20 % Snappy / 30 % Zstd L3 / 10 % GDeflate (pages <= 64 KiB)",
             "latency": "submit to completion, measured by the server"}
+
+
+def run_reference_gpu(torch, batch, caps, raws, stream, flush, steps, warm, alg_bytes):
+    """The reference library's own sm_100a LZ4 kernel (its src/batch.cu,
+    compiled from its sources into oracle/_ref) on the same device batch,
+    flush and events: the GPU kernel this library is measured against. A
+    baseline leg outside the headline timed region."""
+    import oracle
+    ref = oracle.ref_gpu_lib()
+    if ref is None:
+        return {"unavailable": "reference library not built (oracle/_ref/libcudec_ref.so)"}
+
+    def body():
+        assert ref.cudec_lz4_decompress_batch(*batch.args(), stream.cuda_stream) == 0
+
+    with torch.cuda.stream(stream):
+        body()
+    stream.synchronize()
+    res = batch.results()
+    assert (res["status"] == 0).all() and (res["bytes_written"] == np.array(caps)).all()
+    verified = verify_outputs(batch, caps, expect=raws)
+    ms = time_region(torch, stream, flush, steps, warm, body)
+    out = float(sum(caps))
+    return {"value": round(out / (ms * 1e-3) / 1e9, 3), "unit": "GB/s",
+            "ms_per_step": round(ms, 5), "steps": steps, "verified_chunks": verified,
+            "roofline_frac": round(alg_bytes / (ms * 1e-3) / 1e9 / peaks()[0], 5),
+            "kernel": "reference lz4_decode_batch<false> (src/lz4_decode.cuh:29-173) "
+                      "built for sm_100a, through its cudec_lz4_decompress_batch"}
+
+
+def pyarrow_version():
+    import pyarrow
+    return pyarrow.__version__
+
+
+def snappy_cpu(comps, caps, seconds, threads):
+    """snappy's raw decompressor (bundled in pyarrow; it releases the GIL)
+    over the batch from a thread pool, for ~`seconds`."""
+    from concurrent.futures import ThreadPoolExecutor
+    from cudec_b200 import workload as W
+    codec = W.snappy_codec()
+
+    def one(k):
+        return codec.decompress(comps[k], decompressed_size=caps[k])
+
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        outs = list(ex.map(one, range(len(comps))))
+        assert all(o.size == c for o, c in zip(outs, caps))
+        reps, t0 = 0, time.perf_counter()
+        while True:
+            for _ in ex.map(one, range(len(comps)), chunksize=16):
+                pass
+            reps += 1
+            el = time.perf_counter() - t0
+            if el >= seconds:
+                break
+    return float(sum(caps)) * reps / el / 1e9, threads, reps
 
 
 def time_device(torch, batch, fmt, stream, flush, steps, warmup):
@@ -504,6 +629,10 @@ def main():
         run_reference(args, rank)
         return
 
+    # Zstd / GDeflate inputs are compressed on all host cores while the
+    # device legs below run (spawned workers, started before CUDA is used)
+    gen_pool, gen_jobs = start_generation(args)
+
     import torch
     import torch.distributed as dist
     import cudec_b200 as cd
@@ -530,9 +659,7 @@ def main():
     stream.synchronize()
     res = batch.results()
     assert (res["status"] == 0).all() and (res["bytes_written"] == CHUNK).all()
-    dst = batch.dst_host()
-    for i in range(0, n, 97):
-        assert batch.output(i, dst, CHUNK) == raws[i].tobytes()
+    verified = verify_outputs(batch, caps, expect=raws)
 
     def barrier():
         if world > 1:
@@ -548,6 +675,15 @@ def main():
         barrier()
     mean_ms = max_over_ranks(mean_ms)
     value = world * out_bytes / (mean_ms * 1e-3) / 1e9
+    res = batch.results()
+    assert (res["status"] == 0).all() and (res["bytes_written"] == CHUNK).all()
+    assert verify_outputs(batch, caps, expect=raws) == n
+
+    # ---- the reference's own kernel on the same batch (a baseline leg) --
+    ref_gpu = None
+    if world == 1 and rank == 0:
+        ref_gpu = run_reference_gpu(torch, batch, caps, raws, stream, flush,
+                                    max(args.steps // 4, 3), warm, in_bytes + out_bytes)
 
     # ---- Snappy, same content -------------------------------------------
     _, scomps = workload(n, "snappy")
@@ -555,7 +691,8 @@ def main():
     s_ms = max_over_ranks(time_device(torch, sbatch, "snappy", stream, flush,
                                       max(args.steps // 4, 1), warm))
     sres = sbatch.results()
-    assert (sres["status"] == 0).all()
+    assert (sres["status"] == 0).all() and (sres["bytes_written"] == CHUNK).all()
+    s_verified = verify_outputs(sbatch, caps, expect=raws)
     s_in = sum(len(c) for c in scomps)
     del sbatch
 
@@ -565,43 +702,47 @@ def main():
         mixed_line = run_mixed(torch, cd, DeviceBatch, args, dev, stream, flush,
                                max_over_ranks, world, warm)
 
-    # ---- GDeflate pages (TileStream tiles) ------------------------------
-    gd_line = None
-    if args.gdeflate_streams > 0:
-        gd_line = run_gdeflate(torch, cd, DeviceBatch, args, dev, stream, flush,
-                               max_over_ranks, world, warm)
-
     # ---- served stream: continuous batching vs the plain queue --------
     serve_line = None
     if args.serve_requests > 0:
         serve_line = run_serve(cd, args, dev)
 
+    # ---- GDeflate pages (TileStream tiles) ------------------------------
+    gd_line = None
+    if args.gdeflate_streams > 0:
+        gd_line = run_gdeflate(torch, cd, DeviceBatch, args, dev, stream, flush,
+                               max_over_ranks, world, warm, gen_jobs["gdeflate"].get())
+
     # ---- Zstd, 1 MiB frames at levels 3 and 19 ------------------------
     zstd_lines = {}
+    zstd_sample = None
     if args.zstd_frames > 0:
         for level in (3, 19):
-            zraws, zuniq = zstd_workload(min(args.zstd_unique, args.zstd_frames), level)
+            made = gen_jobs["zstd_l%d" % level].get()
+            zdig, zuniq = [m[0] for m in made], [m[1] for m in made]
             zn = args.zstd_frames
             zcomps = [zuniq[i % len(zuniq)] for i in range(zn)]
+            if level == 3:
+                zstd_sample = zuniq[:256]
             zbatch = DeviceBatch(zcomps, [ZSTD_FRAME] * zn, device=dev, poison=None)
             z_ms = max_over_ranks(time_device(torch, zbatch, "zstd", stream, flush,
                                               max(args.steps // 20, 3), warm))
             zres = zbatch.results()
             assert (zres["status"] == 0).all() and (zres["bytes_written"] == ZSTD_FRAME).all()
-            zdst = zbatch.dst_host() if zn <= 1024 else None
-            for i in range(0, zn, max(zn // 16, 1)):
-                got = zbatch.output(i, zdst, ZSTD_FRAME) if zdst is not None else \
-                    zbatch.d_dst[int(zbatch.dst_offs[i]):int(zbatch.dst_offs[i]) + ZSTD_FRAME].cpu().numpy().tobytes()
-                assert got == zraws[i % len(zraws)]
+            zver = verify_outputs(zbatch, [ZSTD_FRAME] * zn,
+                                  digests=[zdig[i % len(zdig)] for i in range(zn)])
             z_in = zbatch.src_bytes
             z_out = ZSTD_FRAME * zn
             zstd_lines["zstd_l%d" % level] = {
                 "value": round(world * z_out / (z_ms * 1e-3) / 1e9, 3),
                 "ms_per_step": round(z_ms, 4), "frames": zn, "unique_frames": len(zuniq),
+                "verified_chunks": zver,
                 "frame_bytes": ZSTD_FRAME, "compressed_bytes": z_in,
                 "roofline_frac": round((z_in + z_out) / (z_ms * 1e-3) / 1e9 / peaks()[0], 5)}
             del zbatch
             torch.cuda.empty_cache()
+    if gen_pool is not None:
+        gen_pool.join()
 
     # ---- end to end through the C ABI with host buffers ----------------
     # cudec_lz4_decompress_stream_ctx: compressed chunks in pinned host memory
@@ -637,9 +778,7 @@ def main():
             if k >= warm:
                 times.append(t1 - t0)
         ctx.close()
-        dst = batch.dst_host()
-        for i in range(0, n, 101):
-            assert batch.output(i, dst, CHUNK) == raws[i].tobytes()
+        assert verify_outputs(batch, caps, expect=raws) == n
         return max_over_ranks(1e3 * sum(times) / len(times))
 
     e2e_staged_ms = e2e_ms_for(staged_ptrs_h)
@@ -657,6 +796,7 @@ def main():
             "dtype": "u8", "data": "synthetic",
             "config": {"workload": WORKLOAD % n, "format": "lz4", "chunks": n,
                        "chunk_bytes": CHUNK, "compressed_bytes": in_bytes,
+                       "verified_chunks": verified,
                        "parallelism": "replicas x%d" % world,
                        "l2": "flushed before every timed launch (256 MiB memset)"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
@@ -675,11 +815,12 @@ def main():
             "per_format": {
                 "lz4": {"value": round(value, 3), "ms_per_step": round(mean_ms, 5)},
                 "snappy": {"value": round(world * out_bytes / (s_ms * 1e-3) / 1e9, 3),
-                           "ms_per_step": round(s_ms, 5),
+                           "ms_per_step": round(s_ms, 5), "verified_chunks": s_verified,
                            "roofline_frac": round((s_in + out_bytes) / (s_ms * 1e-3) / 1e9 / peak, 5)},
                 **zstd_lines,
                 **({"gdeflate": gd_line} if gd_line else {}),
             },
+            **({"reference_gpu": ref_gpu} if ref_gpu else {}),
             **({"mixed": mixed_line} if mixed_line else {}),
             **({"serve": serve_line} if serve_line else {}),
             "gpu_launches": args.steps,
@@ -695,10 +836,27 @@ def main():
                 "kind": "reference" if kind == "ref_lz4" else "port",
                 "sample": "%d passes over the same %d x 64 KiB batch (~%.0f s); reference "
                           "twin tests/lz4_twin.h on a std::thread pool" % (reps, n, args.cpu_seconds)}
-            cv, cused, _ = cpu_sample("codec_lz4", comps, caps, min(args.cpu_seconds, 5.0), threads)
+            csec = min(args.cpu_seconds, 5.0)
+            cv, cused, _ = cpu_sample("codec_lz4", comps, caps, csec, threads)
             line["cpu_codec"] = {"value": round(cv, 3), "unit": "GB/s", "cores": cused,
                                  "library": "liblz4 %d LZ4_decompress_safe"
                                             % oracle.oracle_lib().codec_lz4_version()}
+            # the same measurement for the other formats' codec libraries
+            sv, sused, sreps = snappy_cpu(scomps, caps, csec, threads)
+            line["per_format"]["snappy"]["cpu_codec"] = {
+                "value": round(sv, 3), "unit": "GB/s", "cores": sused,
+                "library": "snappy (pyarrow %s) raw decompress, one call per chunk on a "
+                           "thread pool" % pyarrow_version(),
+                "sample": "%d passes over the %d x 64 KiB batch" % (sreps, n)}
+            if zstd_sample:
+                zv, zused, zreps = cpu_sample("codec_zstd", zstd_sample,
+                                              [ZSTD_FRAME] * len(zstd_sample), csec, threads)
+                line["per_format"]["zstd_l3"]["cpu_codec"] = {
+                    "value": round(zv, 3), "unit": "GB/s", "cores": zused,
+                    "library": "libzstd %d ZSTD_decompressDCtx, one DCtx per thread"
+                               % oracle.oracle_lib().codec_zstd_version(),
+                    "sample": "%d passes over %d of the level-3 1 MiB frames"
+                              % (zreps, len(zstd_sample))}
         print(json.dumps(line), flush=True)
     replicas.finish()
 

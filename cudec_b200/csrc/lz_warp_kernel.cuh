@@ -994,6 +994,12 @@ __device__ __forceinline__ int parse_chunk(const uint8_t* g, uint64_t S, uint64_
     uint64_t d = 0;  // output position of the next token
     LZW_T(t_chunk);
     uint64_t refill_at = 0;
+    // Fuel: every token consumes at least one source byte, so a chunk of S
+    // bytes holds at most S + 1 tokens (saturating at the top of the range).
+    // No input reaches the cap; it turns a parser fault into a rejected
+    // chunk instead of a warp that never leaves this loop (the reference's
+    // cap, src/lz4_decode.cuh:99,152). m is warp-uniform, so the test is too.
+    uint64_t fuel = S == ~0ull ? ~0ull : S + 1;
     for (;;) {
         LZW_T(t_land);
         if (p >= refill_at) {
@@ -1041,6 +1047,11 @@ __device__ __forceinline__ int parse_chunk(const uint8_t* g, uint64_t S, uint64_
             m = k + 1;
             last = true;
         }
+        if (m > fuel) {
+            status = CUDEC_ERR_CORRUPT_INPUT;
+            break;
+        }
+        fuel -= m;
         const uint64_t tend = dl + sq.lit + sq.ml;
         const uint64_t nxt = __shfl_sync(kFull, sq.next, m - 1);
         const uint64_t dend = __shfl_sync(kFull, tend, m - 1);

@@ -146,7 +146,11 @@ cudec_status cudec_zstd_decompress_batch(const void* const* d_src_ptrs,
  * CUDEC_ERR_INVALID_ARGUMENT, returned before any CUDA call. The array is
  * shared by every call on a device: calls whose launches overlap in time
  * (different streams or host threads) race on it; calls queued on one stream
- * are ordered and safe. */
+ * are ordered and safe. The first call on a device looks up the array's
+ * device address (once per device, with that device current), so make that
+ * first call before any stream capture. The address is kept for the life of
+ * the process: after cudaDeviceReset on a device, this entry must not be
+ * called on it again until the library is reloaded. */
 #define CUDEC_ZSTD_NOALLOC_MAX_CHUNKS 64
 
 cudec_status cudec_zstd_decompress_batch_noalloc(const void* const* d_src_ptrs,

@@ -27,10 +27,12 @@ _DEC = [_U8P, _U64, _U8P, _U64, ctypes.POINTER(_U64)]
 _BATCH = [_U8P, _U8P, _U8P, _U8P, _U64, _U8P, _U8P, ctypes.c_int]
 
 
-def build():
-    """Compile the restatement (and the reference pieces when its tree is
-    present) with oracle/Makefile."""
-    subprocess.run(["make", "-s", "-f", os.path.join(HERE, "Makefile")],
+def build(ref=None):
+    """Compile the restatement with oracle/Makefile, and the reference pieces
+    when `ref` (or the CUDEC_REFERENCE environment variable) names the
+    reference tree."""
+    ref = ref or os.environ.get("CUDEC_REFERENCE", "")
+    subprocess.run(["make", "-s", "-f", os.path.join(HERE, "Makefile"), "REF=" + ref],
                    check=True)
 
 

@@ -1,9 +1,9 @@
 """Generate the golden fixtures for the LZ4 and Snappy block parity tests.
 
-Run in a container where the reference tree is mounted (path below, or
-CUDEC_REFERENCE) and oracle/_ref has been built (`make -f oracle/Makefile`):
+Run where the reference tree is mounted, with CUDEC_REFERENCE naming it,
+after oracle/_ref has been built (`make -f oracle/Makefile REF=<tree>`):
 
-    python tests/golden/make_golden.py
+    CUDEC_REFERENCE=<tree> python tests/golden/make_golden.py
 
 Sources of the vectors:
   * the reference's own fuzz seeds, fuzz/corpus/fuzz_lz4_block/* (framing:
@@ -31,7 +31,7 @@ sys.path.insert(0, ROOT)
 import oracle  # noqa: E402
 from cudec_b200 import workload  # noqa: E402
 
-REF = os.environ.get("CUDEC_REFERENCE", "/root/reference")
+REF = os.environ.get("CUDEC_REFERENCE", "")
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -207,6 +207,8 @@ def _declared(body):
 
 
 def main():
+    if not REF or not os.path.isdir(os.path.join(REF, "fuzz")):
+        sys.exit("CUDEC_REFERENCE must name the reference tree")
     if oracle.ref_twin_lib() is None:
         sys.exit("oracle/_ref/libref_twin.so missing: run make -f oracle/Makefile")
     for name, vecs in (("lz4_block.json", lz4_vectors()),
