@@ -1,4 +1,5 @@
-// C-ABI batch entries for the byte-oriented LZ formats (LZ4, raw Snappy).
+// C-ABI batch entries for the byte-oriented LZ formats (LZ4, raw Snappy):
+// the CTA-per-chunk decoder (lz_cta_kernel.cuh), persistent over the batch.
 //
 // Contract (include/cudec.h): synchronous validation with no CUDA call on a
 // reject, then the pending CUDA error is consumed, the kernel is submitted on
@@ -12,7 +13,7 @@
 
 #include "cudec.h"
 #include "launch.h"
-#include "lz_warp_kernel.cuh"
+#include "lz_cta_kernel.cuh"
 
 namespace cdb {
 
@@ -30,34 +31,8 @@ cudec_status validate_batch(const void* const* src, const size_t* src_sizes,
 
 namespace {
 
-// Per-device one-time setup: the kernels use more than 48 KB of dynamic
-// shared memory (opted into once per device and kernel), and the persistent
-// grid is at most the resident CTAs per SM times the SM count.
 constexpr int kMaxDevices = 64;
-std::atomic<int> g_lz4_ready[kMaxDevices];
-std::atomic<int> g_snappy_ready[kMaxDevices];
 std::atomic<int> g_sm_count[kMaxDevices];
-
-template <class Fmt>
-cudaError_t prepare(std::atomic<int>* ready, int dev, int* per_sm) {
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    int v = ready[dev].load(std::memory_order_acquire);
-    if (v > 0) {
-        *per_sm = v;
-        return cudaSuccess;
-    }
-    constexpr int kSmem = static_cast<int>(lzw::kWarps * lzw::kWarpSmem);
-    cudaError_t e = cudaFuncSetAttribute(lzw::lz_warp_kernel<Fmt>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
-    if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, lzw::lz_warp_kernel<Fmt>,
-                                                      lzw::kThreads, kSmem);
-    if (e != cudaSuccess) return e;
-    if (v <= 0) return cudaErrorInvalidConfiguration;
-    ready[dev].store(v, std::memory_order_release);
-    *per_sm = v;
-    return cudaSuccess;
-}
 
 }  // namespace
 
@@ -71,26 +46,50 @@ int device_sm_count(int dev) {
     return v;
 }
 
-template <class Fmt>
-static cudec_status launch_lz(std::atomic<int>* ready, const void* const* src,
-                              const size_t* src_sizes, void* const* dst,
-                              const size_t* caps, size_t n,
-                              cudec_chunk_result* results,
-                              cudaStream_t stream) {
+// The CTA-per-chunk kernel's resident CTAs per SM, once per device and
+// format (its shared state exceeds 48 KB: opted into here).
+template <class F>
+cudaError_t prepare_cta(std::atomic<int>* ready, int dev, int* per_sm) {
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    int v = ready[dev].load(std::memory_order_acquire);
+    if (v > 0) {
+        *per_sm = v;
+        return cudaSuccess;
+    }
+    constexpr int kSmem = static_cast<int>(sizeof(lzc::Shm<F>));
+    cudaError_t e = cudaFuncSetAttribute(lzc::lz_cta_kernel<F>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, lzc::lz_cta_kernel<F>, lzc::kThreads,
+                                                      kSmem);
+    if (e != cudaSuccess) return e;
+    if (v <= 0) return cudaErrorInvalidConfiguration;
+    ready[dev].store(v, std::memory_order_release);
+    *per_sm = v;
+    return cudaSuccess;
+}
+
+std::atomic<int> g_lz4_cta_ready[kMaxDevices];
+std::atomic<int> g_snappy_cta_ready[kMaxDevices];
+
+// One CTA per chunk at a time, persistent over the batch.
+template <class F>
+static cudec_status launch_lz_cta(std::atomic<int>* ready, const void* const* src,
+                                  const size_t* src_sizes, void* const* dst, const size_t* caps,
+                                  size_t n, cudec_chunk_result* results, cudaStream_t stream) {
     const cudec_status v = validate_batch(src, src_sizes, dst, caps, n, results);
     if (v != CUDEC_OK) return v;
     (void)cudaGetLastError();
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return CUDEC_ERR_CUDA;
     int per_sm = 0;
-    if (prepare<Fmt>(ready, dev, &per_sm) != cudaSuccess) return CUDEC_ERR_CUDA;
+    if (prepare_cta<F>(ready, dev, &per_sm) != cudaSuccess) return CUDEC_ERR_CUDA;
     const int sms = device_sm_count(dev);
     if (sms <= 0) return CUDEC_ERR_CUDA;
     const size_t max_blocks = static_cast<size_t>(sms) * per_sm;
-    const size_t want = (n + lzw::kWarps - 1) / lzw::kWarps;
-    const unsigned grid = static_cast<unsigned>(want < max_blocks ? want : max_blocks);
-    lzw::lz_warp_kernel<Fmt><<<grid, lzw::kThreads, lzw::kWarps * lzw::kWarpSmem, stream>>>(
-        src, src_sizes, dst, caps, n, results, lzw::kDefaultTune);
+    const unsigned grid = static_cast<unsigned>(n < max_blocks ? n : max_blocks);
+    lzc::lz_cta_kernel<F><<<grid, lzc::kThreads, sizeof(lzc::Shm<F>), stream>>>(
+        src, src_sizes, dst, caps, n, results);
     return cudaGetLastError() == cudaSuccess ? CUDEC_OK : CUDEC_ERR_CUDA;
 }
 
@@ -105,8 +104,8 @@ cudec_status cudec_lz4_decompress_batch(const void* const* d_src_ptrs,
                                         size_t chunk_count,
                                         cudec_chunk_result* d_results,
                                         cudec_stream_t stream) {
-    return cdb::launch_lz<cdb::lzw::Lz4>(
-        cdb::g_lz4_ready, d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_capacities,
+    return cdb::launch_lz_cta<cdb::lzc::Lz4F>(
+        cdb::g_lz4_cta_ready, d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_capacities,
         chunk_count, d_results, reinterpret_cast<cudaStream_t>(stream));
 }
 
@@ -117,8 +116,8 @@ cudec_status cudec_snappy_decompress_batch(const void* const* d_src_ptrs,
                                            size_t chunk_count,
                                            cudec_chunk_result* d_results,
                                            cudec_stream_t stream) {
-    return cdb::launch_lz<cdb::lzw::Snappy>(
-        cdb::g_snappy_ready, d_src_ptrs, d_src_sizes, d_dst_ptrs,
+    return cdb::launch_lz_cta<cdb::lzc::SnappyF>(
+        cdb::g_snappy_cta_ready, d_src_ptrs, d_src_sizes, d_dst_ptrs,
         d_dst_capacities, chunk_count, d_results,
         reinterpret_cast<cudaStream_t>(stream));
 }

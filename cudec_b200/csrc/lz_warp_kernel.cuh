@@ -40,6 +40,7 @@
 #include <cstdint>
 
 #include "cudec.h"
+#include "lz_ladder.cuh"
 
 namespace cdb {
 namespace lzw {
@@ -95,14 +96,7 @@ __device__ unsigned long long lzw_events[8];
 #define LZW_EV(i, n)
 #endif
 
-// One parsed sequence: lit literal bytes from input offset lit_src, then ml
-// bytes copied from off bytes back; next = the following token's position;
-// done = the chunk ends after this sequence (LZ4's terminal literal run).
-struct Seq {
-    uint64_t lit_src, lit, ml, next;
-    uint32_t off;
-    bool done;
-};
+using Seq = lzl::Seq;
 
 __device__ __forceinline__ uint32_t ldb(const uint8_t* g, uint64_t p) {
     return __ldg(g + p);
@@ -111,6 +105,13 @@ __device__ __forceinline__ uint32_t ldb(const uint8_t* g, uint64_t p) {
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
+
+// The chunk's bytes straight from global memory (the ladders' reader for a
+// chunk's preamble).
+struct GBytes {
+    const uint8_t* g;
+    __device__ __forceinline__ uint32_t at(uint64_t q) const { return ldb(g, q); }
+};
 
 // The chunk's compressed bytes: positions in [lo, lo + span) come from the
 // shared-memory window (indexed by global address mod kIn, so its 16-byte
@@ -132,37 +133,8 @@ struct In {
 };
 
 // ---------------------------------------------------------------------------
-// LZ4 block (src/lz4_block.h:139-258 Lz4Parser::Next, :95-128
-// AccumulateLength; constants :46-66).
-struct Lz4 {
-    static constexpr uint64_t kMfLimit = 12;
-    static constexpr uint64_t kSrcSlack = 8;
-    static constexpr uint64_t kLastLiterals = 5;
-
-    __device__ static int begin(const uint8_t*, uint64_t, uint64_t cap, uint64_t* first,
-                                uint64_t* limit) {
-        *first = 0;
-        *limit = cap;
-        return CUDEC_OK;
-    }
-    __device__ __forceinline__ static bool at_end(uint64_t, uint64_t) { return false; }
-    __device__ __forceinline__ static int finish(uint64_t, uint64_t) { return CUDEC_OK; }
-
-    __device__ __forceinline__ static int extend(const In& in, uint64_t S, uint64_t* q,
-                                                 uint64_t* len, uint64_t room, uint64_t margin,
-                                                 bool pre) {
-        if (pre && *q + margin >= S) return CUDEC_ERR_CORRUPT_INPUT;
-        uint32_t b;
-        do {
-            if (*q >= S) return CUDEC_ERR_CORRUPT_INPUT;
-            if (*len > room) return CUDEC_ERR_OUTPUT_TOO_SMALL;
-            b = in.at((*q)++);
-            *len += b;
-            if (*q + margin > S) return CUDEC_ERR_CORRUPT_INPUT;
-        } while (b == 255);
-        return CUDEC_OK;
-    }
-
+// LZ4 block: the exact ladder (lz_ladder.cuh) plus the group walk's steps.
+struct Lz4 : lzl::Lz4Ladder {
     // The group walk reads token headers from the landed window only: r is a
     // position relative to the group's first token, its window slot is
     // (gb + r) & (kIn - 1), and e bounds what may be read (the input end or
@@ -227,79 +199,11 @@ struct Lz4 {
         return q;
     }
 
-    // The token at p with d bytes already produced; cap is the capacity.
-    __device__ __forceinline__ static int parse(const In& in, uint64_t S, uint64_t cap,
-                                                uint64_t p, uint64_t d, Seq* s) {
-        if (p >= S) return CUDEC_ERR_CORRUPT_INPUT;
-        const uint32_t tok = in.at(p);
-        uint64_t q = p + 1;
-        uint64_t lit = tok >> 4;
-        if (lit == 15) {
-            const int st = extend(in, S, &q, &lit, cap - d, 15, true);
-            if (st != CUDEC_OK) return st;
-        }
-        if (lit > S - q) return CUDEC_ERR_CORRUPT_INPUT;
-        if (lit > cap - d) return CUDEC_ERR_OUTPUT_TOO_SMALL;
-        s->lit_src = q;
-        s->lit = lit;
-        if (cap - d - lit < kMfLimit || S - q - lit < kSrcSlack) {
-            if (q + lit != S) return CUDEC_ERR_CORRUPT_INPUT;
-            // Capacity zero accepts only the single byte 0x00 (lz4_block.h:178-187).
-            if (cap == 0 && tok != 0) return CUDEC_ERR_CORRUPT_INPUT;
-            s->ml = 0;
-            s->off = 0;
-            s->next = S;
-            s->done = true;
-            return CUDEC_OK;
-        }
-        q += lit;
-        d += lit;
-        const uint32_t off = in.at(q) | (in.at(q + 1) << 8);
-        q += 2;
-        if (off == 0) return CUDEC_ERR_CORRUPT_INPUT;  // stricter than liblz4
-        if (off > d) return CUDEC_ERR_CORRUPT_INPUT;
-        uint64_t ml = (tok & 15) + 4;
-        if ((tok & 15) == 15) {
-            const int st = extend(in, S, &q, &ml, cap - d, 4, false);
-            if (st != CUDEC_OK) return st;
-        }
-        if (ml > cap - d) return CUDEC_ERR_OUTPUT_TOO_SMALL;
-        if (ml > cap - d - kLastLiterals) return CUDEC_ERR_CORRUPT_INPUT;
-        s->ml = ml;
-        s->off = off;
-        s->next = q;
-        s->done = false;
-        return CUDEC_OK;
-    }
 };
 
 // ---------------------------------------------------------------------------
-// Raw Snappy (src/snappy_block.h:172-223 SnappyDeclaredLength, :249-435
-// SnappyParser::Begin/Next). One element (literal OR copy) per Seq.
-struct Snappy {
-    __device__ static int begin(const uint8_t* g, uint64_t S, uint64_t cap, uint64_t* first,
-                                uint64_t* limit) {
-        uint64_t v = 0;
-        for (uint64_t k = 0; k < 5; ++k) {
-            if (k >= S) return CUDEC_ERR_CORRUPT_INPUT;
-            const uint32_t b = ldb(g, k);
-            if (k == 4 && b >= 16) return CUDEC_ERR_CORRUPT_INPUT;
-            v |= static_cast<uint64_t>(b & 0x7f) << (7 * k);
-            if (!(b & 0x80)) {
-                if (v > cap) return CUDEC_ERR_OUTPUT_TOO_SMALL;
-                *first = k + 1;
-                *limit = v;
-                return CUDEC_OK;
-            }
-        }
-        return CUDEC_ERR_CORRUPT_INPUT;
-    }
-    __device__ __forceinline__ static bool at_end(uint64_t p, uint64_t S) { return p == S; }
-    // Elements exhausted: success only at exact production of the declared length.
-    __device__ __forceinline__ static int finish(uint64_t d, uint64_t declared) {
-        return d == declared ? CUDEC_OK : CUDEC_ERR_CORRUPT_INPUT;
-    }
-
+// Raw Snappy: the exact ladder (lz_ladder.cuh) plus the group walk's steps.
+struct Snappy : lzl::SnappyLadder {
     // Branch-free step for tags whose length is in the tag (see
     // Lz4::step_simple). Strict bound: an element ending at e may end the
     // input, which only the general step (with its end check) decides.
@@ -344,54 +248,6 @@ struct Snappy {
         return r + hdr;
     }
 
-    __device__ __forceinline__ static int parse(const In& in, uint64_t S,
-                                                uint64_t declared, uint64_t p, uint64_t d,
-                                                Seq* s) {
-        const uint32_t tag = in.at(p);
-        const uint32_t kind = tag & 3;
-        s->done = false;
-        if (kind == 0) {
-            const uint32_t l6 = tag >> 2;
-            uint64_t hdr = 1, len = l6;
-            if (l6 >= 60) {
-                const uint32_t extra = l6 - 59;
-                hdr += extra;
-                if (hdr > S - p) return CUDEC_ERR_CORRUPT_INPUT;
-                len = 0;
-                for (uint32_t i = 0; i < extra; ++i)
-                    len |= static_cast<uint64_t>(in.at(p + 1 + i)) << (8 * i);
-            }
-            len += 1;  // 64-bit: the 0xFFFFFFFF spelling is refused, not wrapped
-            const uint64_t q = p + hdr;
-            if (len > S - q) return CUDEC_ERR_CORRUPT_INPUT;
-            if (len > declared - d) return CUDEC_ERR_CORRUPT_INPUT;
-            s->lit_src = q;
-            s->lit = len;
-            s->ml = 0;
-            s->off = 0;
-            s->next = q + len;
-            return CUDEC_OK;
-        }
-        const uint32_t ob = kind == 1 ? 1 : (kind == 2 ? 2 : 4);
-        if (1 + ob > S - p) return CUDEC_ERR_CORRUPT_INPUT;
-        uint64_t off = 0, len;
-        for (uint32_t i = 0; i < ob; ++i) off |= static_cast<uint64_t>(in.at(p + 1 + i)) << (8 * i);
-        if (kind == 1) {
-            off |= static_cast<uint64_t>(tag >> 5) << 8;
-            len = 4 + ((tag >> 2) & 7);
-        } else {
-            len = (tag >> 2) + 1;
-        }
-        if (off == 0) return CUDEC_ERR_CORRUPT_INPUT;
-        if (off > d) return CUDEC_ERR_CORRUPT_INPUT;
-        if (len > declared - d) return CUDEC_ERR_CORRUPT_INPUT;
-        s->lit_src = p;
-        s->lit = 0;
-        s->ml = len;
-        s->off = static_cast<uint32_t>(off);
-        s->next = p + 1 + ob;
-        return CUDEC_OK;
-    }
 };
 
 // ---------------------------------------------------------------------------
@@ -548,12 +404,16 @@ struct Out {
     __device__ __forceinline__ void flush(uint64_t end, bool final, uint32_t lane) {
         const uint64_t f = flushed;
         if (end <= f) return;
-        uint64_t fa = ((dbase + f + 15) & ~static_cast<uintptr_t>(15)) - dbase;
-        const uint64_t ea = ((dbase + end) & ~static_cast<uintptr_t>(15)) - dbase;
-        const uint64_t hend = fa < end ? fa : end;
+        // in addresses: the first aligned boundary at or after f, the last at
+        // or before end (the latter may lie below the former when [f, end)
+        // sits inside one partial block)
+        const uintptr_t fa_abs = (dbase + f + 15) & ~static_cast<uintptr_t>(15);
+        const uintptr_t ea_abs = (dbase + end) & ~static_cast<uintptr_t>(15);
+        const uint64_t hend = (fa_abs < dbase + end ? fa_abs : dbase + end) - dbase;
         if (f + lane < hend) dst[f + lane] = ring[idx(f + lane)];
         uint64_t nf = hend;
-        if (ea > fa) {
+        if (ea_abs > fa_abs) {
+            const uint64_t fa = fa_abs - dbase, ea = ea_abs - dbase;
             for (uint64_t b = fa + 16ull * lane; b < ea; b += 16ull * 32)
                 *reinterpret_cast<uint4*>(dst + b) = *reinterpret_cast<const uint4*>(ring + idx(b));
             nf = ea;
@@ -983,7 +843,7 @@ __device__ __forceinline__ int parse_chunk(const uint8_t* g, uint64_t S, uint64_
                                            Sink& sink, In& in, uint64_t* dend_out) {
     *dend_out = 0;
     uint64_t p, limit;
-    int status = F::begin(g, S, cap, &p, &limit);
+    int status = F::begin(GBytes{g}, S, cap, &p, &limit);
     if (status != CUDEC_OK) return status;
 
     const uintptr_t gbase = reinterpret_cast<uintptr_t>(g);

@@ -103,6 +103,22 @@ def test_unaligned_buffers(cuda, fmt, skew):
 
 
 @pytest.mark.parametrize("fmt", ["lz4", "snappy"])
+def test_tiny_outputs_at_every_alignment(cuda, fmt):
+    """Outputs shorter than a 16-byte block, and a little longer, at every
+    destination misalignment: the whole output can sit inside the first
+    partial block, where the aligned part of a flush is empty."""
+    rng = random.Random(5)
+    raws = [bytes(rng.randrange(4) + 97 for _ in range(n))
+            for n in (1, 2, 3, 5, 8, 11, 12, 13, 15, 16, 17, 20, 31, 33, 47)]
+    comps = [COMPRESS[fmt](r) for r in raws]
+    caps = [len(r) for r in raws]
+    for skew in range(16):
+        b, res, dst = run_batch(cuda, fmt, comps, caps, dst_skew=skew, src_skew=(skew * 3) % 16)
+        check_against_oracle(fmt, b, res, dst, comps, caps, "tiny skew %d" % skew)
+        assert all(res["status"] == 0)
+
+
+@pytest.mark.parametrize("fmt", ["lz4", "snappy"])
 def test_short_periods_at_every_alignment(cuda, fmt):
     """Matches whose period is shorter than a 16-byte vector, starting in the
     first vectors of the destination, for every destination misalignment."""
