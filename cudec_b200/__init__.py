@@ -67,6 +67,8 @@ SIGNATURES = {
     "cudec_server_destroy": (ctypes.c_int, [_P]),
     "cudec_server_submit": (ctypes.c_int, [_P, _P, _SZ, _P, _P, _P, _P, _SZ, _P]),
     "cudec_server_wait": (ctypes.c_int, [_P, ctypes.c_uint64, _P, _P, _P]),
+    "cudec_server_wait_for": (ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_double, _P, _P, _P,
+                                             _P]),
     "cudec_server_release": (ctypes.c_int, [_P, ctypes.c_uint64]),
     "cudec_lz4f_decompress": (ctypes.c_int, [_P, _SZ, _P, _SZ, _P]),
     "cudec_stream_ctx_create": (ctypes.c_int, [_P]),
@@ -308,6 +310,21 @@ class Server:
         st = lib().cudec_server_wait(self.handle, ticket, recs.ctypes.data, ptrs.ctypes.data,
                                      ctypes.byref(lat))
         return st, recs, ptrs, lat.value
+
+    def wait_for(self, ticket, timeout_ms):
+        """Bounded wait: (status, done, records, device output addresses,
+        latency_ms); done False means the deadline passed first."""
+        import numpy as np
+        n = self._keep[ticket][1]
+        recs = np.zeros(n, dtype=[("status", "<i4"), ("reserved", "<u4"),
+                                  ("bytes_written", "<u8")])
+        ptrs = np.zeros(n, dtype=np.uint64)
+        lat = ctypes.c_double()
+        done = ctypes.c_int(-1)
+        st = lib().cudec_server_wait_for(self.handle, ticket, float(timeout_ms),
+                                         ctypes.byref(done), recs.ctypes.data, ptrs.ctypes.data,
+                                         ctypes.byref(lat))
+        return st, bool(done.value == 1), recs, ptrs, lat.value
 
     def release(self, ticket):
         st = lib().cudec_server_release(self.handle, ticket)

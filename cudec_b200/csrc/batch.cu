@@ -123,3 +123,20 @@ cudec_status cudec_snappy_decompress_batch(const void* const* d_src_ptrs,
 }
 
 }  // extern "C"
+
+#ifdef CDB_PHASE_TIMING
+// Profiling builds only: the CTA decoder's phase cycles [0, 16) and event
+// counts [16, 32) since the last call (then reset).
+extern "C" int cudec_lzc_phase_counters(unsigned long long* out) {
+    if (cudaMemcpyFromSymbol(out, cdb::lzc::lzc_cycles, 16 * sizeof(unsigned long long)) !=
+            cudaSuccess ||
+        cudaMemcpyFromSymbol(out + 16, cdb::lzc::lzc_events, 16 * sizeof(unsigned long long)) !=
+            cudaSuccess)
+        return 1;
+    static const unsigned long long zero[16] = {};
+    if (cudaMemcpyToSymbol(cdb::lzc::lzc_cycles, zero, sizeof(zero)) != cudaSuccess ||
+        cudaMemcpyToSymbol(cdb::lzc::lzc_events, zero, sizeof(zero)) != cudaSuccess)
+        return 1;
+    return 0;
+}
+#endif

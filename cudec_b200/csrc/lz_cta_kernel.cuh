@@ -33,10 +33,12 @@
 //   7. execute, in groups of consecutive tokens whose output fits kGroupOut:
 //      the group's literal runs are copied into an output ring in shared
 //      memory (indexed by destination address mod kRing, so ring blocks and
-//      destination blocks share alignment), then its matches in rounds: a
-//      match copies once none of the bytes its source reads is the output of
-//      a match still pending in the group (a bit per output byte); the
-//      lowest pending match is always ready, so every round makes progress.
+//      destination blocks share alignment), then its matches as data flow:
+//      each thread copies each of its matches once none of the bytes its
+//      source reads is the output of a match still pending in the group (a
+//      bit per output byte), and clears the match's own bits after its bytes
+//      land; the lowest pending match is always ready, so the group always
+//      makes progress.
 //      Completed aligned 16-byte blocks leave the ring as coalesced stores.
 //      A token longer than kBig is copied by the whole CTA straight to the
 //      destination. Sources older than the ring are read back from the
@@ -63,6 +65,7 @@ namespace cdb {
 namespace lzc {
 
 constexpr uint32_t kThreads = 256;                 // threads per CTA
+constexpr uint32_t kCtasPerSm = 4;                 // resident CTAs per SM the registers allow
 constexpr uint32_t kWarps = kThreads / 32;
 constexpr uint32_t kSeg = 16;                      // positions per segment (one per thread)
 constexpr uint32_t kTile = kThreads * kSeg;        // positions per tile
@@ -74,11 +77,12 @@ constexpr uint32_t kLook = 512;                    // staged bytes past the tile
 constexpr uint32_t kInBytes = kTile + kLook + 32;  // staged input (aligned blocks)
 constexpr uint32_t kExIdx = kTile + kTile / 16;    // exits, one pad word per 16
 constexpr uint32_t kRing = 16384;                  // output ring (bytes)
-constexpr uint32_t kGroupOut = 8192;               // output bytes per execution group
-constexpr uint32_t kPerThread = 4;                 // tokens per thread per group
+constexpr uint32_t kGroupOut = 4096;               // output bytes per execution group
+constexpr uint32_t kPerThread = 2;                 // tokens per thread per group
 constexpr uint32_t kGroupTok = kThreads * kPerThread;
 constexpr uint32_t kBig = 256;                     // longer tokens: whole-CTA copies
 constexpr uint32_t kExtCap = 16;                   // extension bytes a segment step reads
+constexpr uint32_t kSpinCap = 1u << 22;            // passes a thread makes over its matches
 
 static_assert(kSupers == kWarps, "one super-segment per warp");
 static_assert(kGroupOut + 32 <= kRing, "a group and its clear margin fit the ring");
@@ -92,6 +96,7 @@ constexpr uint32_t kFarRel = 0xFFFFFFF0u;   // relative positions at or above: u
 // Step results (absolute positions otherwise).
 constexpr uint64_t kStepUnknown = ~0ull;
 constexpr uint64_t kStepEnd = ~0ull - 1;
+constexpr uint32_t kSlowRel = 0xFFFFFFFFu;  // a fast step declines: the generic step decides
 
 // Entry codes of the candidate chase (offsets into a segment otherwise).
 constexpr uint8_t kNoEntry = 0xFF;   // no chain token starts in the segment
@@ -119,6 +124,42 @@ inline void at_and(uint32_t* a, uint32_t v) { *a &= v; }
 inline void at_min(uint32_t* a, uint32_t v) {
     if (v < *a) *a = v;
 }
+#endif
+
+// Profiling builds (-DCDB_PHASE_TIMING) accumulate, from thread 0 of every
+// CTA, the SM cycles of each phase and event counts over a launch. Cycles:
+// 0 stage, 1 segment exits, 2 candidate chase, 3 tile chase, 4 count and
+// scan, 5 check, 6 group clear and literals, 7 match rounds, 8 flush,
+// 9 whole-CTA tokens, 10 group cut. Events: 0 tiles, 1 tokens, 2 rounds,
+// 3 groups, 4 whole-CTA tokens, 5 exact walks.
+#if defined(CDB_PHASE_TIMING) && defined(__CUDACC__)
+__device__ unsigned long long lzc_cycles[16];
+__device__ unsigned long long lzc_events[16];
+#endif
+#if defined(CDB_PHASE_TIMING) && defined(__CUDA_ARCH__)
+#define LZC_PHASE(i)                                                                    \
+    do {                                                                                \
+        if (threadIdx.x == 0) {                                                         \
+            const long long n_ = clock64();                                             \
+            atomicAdd(&lzc_cycles[i], static_cast<unsigned long long>(n_ - tl));        \
+            tl = n_;                                                                    \
+        }                                                                               \
+    } while (0)
+#define LZC_EVENT(i, n)                                                                 \
+    do {                                                                                \
+        if (threadIdx.x == 0) atomicAdd(&lzc_events[i], static_cast<unsigned long long>(n)); \
+    } while (0)
+#define LZC_START() tl = clock64()
+#else
+#define LZC_PHASE(i) \
+    do {             \
+    } while (0)
+#define LZC_EVENT(i, n) \
+    do {                \
+    } while (0)
+#define LZC_START() \
+    do {            \
+    } while (0)
 #endif
 
 CDB_HD uint32_t fsr(uint32_t lo, uint32_t hi, uint32_t sh) {  // funnel shift right, sh < 32
@@ -253,6 +294,63 @@ struct Lz4F : lzl::Lz4Ladder {
     CDB_HD static uint64_t lit_src(const R&, uint64_t P, uint64_t lit) {
         return P + 1 + (lit >= 15 ? (lit - 15) / 255 + 1 : 0);
     }
+
+    // Fast forms over the staged bytes, for a token whose header (with at
+    // most kExtCap extension bytes per length) lies well inside them and well
+    // before the chunk's end: b[r] is the token, lim = min(staged bytes, S)
+    // relative to b. kSlowRel: the generic forms decide.
+    static constexpr uint32_t kMargin = 2 * kExtCap + 2 + kSrcSlack;
+    CDB_HD static uint32_t ext_rel(const uint8_t* b, uint32_t* q, uint32_t* len) {
+        for (uint32_t k = 0; k < kExtCap; ++k) {
+            const uint32_t x = b[(*q)++];
+            *len += x;
+            if (x != 255) return 1;
+        }
+        return 0;
+    }
+    CDB_HD static uint32_t step_rel(const uint8_t* b, uint32_t r, uint32_t lim,
+                                    uint32_t* olen) {
+        if (r + kMargin > lim) return kSlowRel;
+        const uint32_t tok = b[r];
+        uint32_t q = r + 1, lit = tok >> 4;
+        if (lit == 15 && !ext_rel(b, &q, &lit)) return kSlowRel;
+        q += lit;
+        if (q + 2 + kExtCap + kSrcSlack > lim) return kSlowRel;
+        q += 2;
+        uint32_t ml = (tok & 15) + 4;
+        if ((tok & 15) == 15 && !ext_rel(b, &q, &ml)) return kSlowRel;
+        *olen = lit + ml;
+        return q;
+    }
+    // The ladder's answer for such a token when it accepts it as
+    // non-terminal: the ladder's conditions (src/lz4_block.h:139-258) on its
+    // final lengths (the extension loops' running checks only fail when the
+    // final values fail them); false: the full ladder decides.
+    CDB_HD static bool accept_rel(const uint8_t* b, uint32_t r, uint32_t lim, uint64_t P,
+                                  uint64_t d, uint64_t cap, lzl::Seq* sq) {
+        if (r + kMargin > lim || cap < d) return false;
+        const uint32_t tok = b[r];
+        uint32_t q = r + 1, lit = tok >> 4;
+        if (lit == 15 && !ext_rel(b, &q, &lit)) return false;
+        const uint32_t ls = q;
+        q += lit;  // the offset's position
+        if (q + 2 + kExtCap + kSrcSlack > lim) return false;
+        const uint32_t off = b[q] | (static_cast<uint32_t>(b[q + 1]) << 8);
+        q += 2;
+        uint32_t ml = (tok & 15) + 4;
+        if ((tok & 15) == 15 && !ext_rel(b, &q, &ml)) return false;
+        const uint64_t room = cap - d;
+        if (lit > room || room - lit < kMfLimit || off == 0 || off > d + lit ||
+            ml + kLastLiterals > room - lit)
+            return false;
+        sq->lit_src = P + (ls - r);
+        sq->lit = lit;
+        sq->ml = ml;
+        sq->off = off;
+        sq->next = P + (q - r);
+        sq->done = false;
+        return true;
+    }
 };
 
 // Raw Snappy: one element per step; an element that ends at S steps to S
@@ -295,6 +393,62 @@ struct SnappyF : lzl::SnappyLadder {
         const uint32_t l6 = tag >> 2;
         return P + 1 + (l6 >= 60 ? l6 - 59 : 0);
     }
+
+    // Fast forms over the staged bytes (see Lz4F): elements whose length
+    // is in the tag; copies with 1- or 2-byte offsets.
+    CDB_HD static uint32_t step_rel(const uint8_t* b, uint32_t r, uint32_t lim,
+                                    uint32_t* olen) {
+        const uint32_t tag = b[r];
+        const uint32_t kind = tag & 3, l6 = tag >> 2;
+        uint32_t nx;
+        if (kind == 0) {
+            if (l6 >= 60) return kSlowRel;
+            nx = r + 2 + l6;
+            *olen = l6 + 1;
+        } else if (kind == 3) {
+            return kSlowRel;
+        } else {
+            nx = r + 1 + kind;
+            *olen = kind == 1 ? 4 + (l6 & 7) : l6 + 1;
+        }
+        return nx <= lim ? nx : kSlowRel;
+    }
+    // The ladder's answer (src/snappy_block.h:249-435) for such an element
+    // when it accepts it; false: the full ladder decides.
+    CDB_HD static bool accept_rel(const uint8_t* b, uint32_t r, uint32_t lim, uint64_t P,
+                                  uint64_t d, uint64_t declared, lzl::Seq* sq) {
+        const uint32_t tag = b[r];
+        const uint32_t kind = tag & 3, l6 = tag >> 2;
+        if (kind == 3 || (kind == 0 && l6 >= 60) || declared < d) return false;
+        const uint64_t room = declared - d;
+        if (kind == 0) {
+            const uint32_t n = l6 + 1;
+            if (r + 1 + n > lim || n > room) return false;
+            sq->lit_src = P + 1;
+            sq->lit = n;
+            sq->ml = 0;
+            sq->off = 0;
+            sq->next = P + 1 + n;
+        } else {
+            if (r + 1 + kind > lim) return false;
+            uint32_t off, len;
+            if (kind == 1) {
+                off = ((tag >> 5) << 8) | b[r + 1];
+                len = 4 + (l6 & 7);
+            } else {
+                off = b[r + 1] | (static_cast<uint32_t>(b[r + 2]) << 8);
+                len = l6 + 1;
+            }
+            if (off == 0 || off > d || len > room) return false;
+            sq->lit_src = P;
+            sq->lit = 0;
+            sq->ml = len;
+            sq->off = off;
+            sq->next = P + 1 + kind;
+        }
+        sq->done = false;
+        return true;
+    }
 };
 
 // ---------------------------------------------------------------------------
@@ -323,8 +477,7 @@ struct Shm {
     uint32_t seg_entry[kThreads];  // relative entry, or kUnknown for none
     uint32_t seg_cnt[kThreads];    // tokens; after the scan, the first token's index
     uint64_t seg_olen[kThreads];   // output bytes; after the scan, the first token's offset
-    uint8_t pend[kThreads];        // per-thread pending match masks (execution rounds)
-    uint8_t done[kThreads];
+    uint8_t pend[kThreads];        // per-thread pending match masks
     uint8_t chosen[kSupers];
     uint32_t wsum_c[kWarps];  // block scan: per-warp totals
     uint64_t wsum_o[kWarps];
@@ -433,15 +586,32 @@ CDB_HD V16 in16(const Reader& in, uint64_t a, uint32_t m) {
 // first 16 bytes' source (low off bytes of v are the period): the match's
 // first 16 bytes. Every later byte repeats the one rest(off) bytes back.
 CDB_HD V16 period16(const V16& v, uint32_t off) {
-    if (off >= 16) return v;
-    uint8_t b[16];
-    for (uint32_t j = 0; j < 16; ++j) b[j] = static_cast<uint8_t>(v.w[j >> 2] >> (8 * (j & 3)));
-    V16 o{{0, 0, 0, 0}};
-    for (uint32_t j = 0; j < 16; ++j) o.w[j >> 2] |= static_cast<uint32_t>(b[j % off]) << (8 * (j & 3));
-    return o;
+    // Without branches, computed in every lane and selected: periods up to 8
+    // bytes doubled in 64 bits, the next 8 bytes starting r = 8 mod off into
+    // the period; for 9..15 bytes the first 16 - off bytes repeat once.
+    const uint64_t lo = (static_cast<uint64_t>(v.w[1]) << 32) | v.w[0];
+    const uint64_t hi = (static_cast<uint64_t>(v.w[3]) << 32) | v.w[2];
+    const uint32_t d = off < 16 ? off : 16u;
+    const uint32_t sb = 8 * d;  // 8..128
+    uint64_t plo = lo & (~0ull >> ((64 - sb) & 63));
+    plo |= sb < 64 ? plo << (sb & 63) : 0ull;
+    plo |= sb < 32 ? plo << ((2 * sb) & 63) : 0ull;
+    plo |= sb < 16 ? plo << ((4 * sb) & 63) : 0ull;
+    // 8 mod d for d = 1..8, one nibble each
+    const uint32_t r = static_cast<uint32_t>((0x012302000ull >> ((4 * d) & 63)) & 15);
+    const uint64_t phi = (plo >> ((8 * r) & 63)) | (plo << ((8 * (d - r)) & 63));
+    const uint32_t s2 = (sb - 64) & 63;
+    const uint64_t qhi = (hi & ((1ull << s2) - 1)) | (lo << s2);
+    const bool small = d <= 8;
+    const uint64_t olo = small ? plo : lo, ohi = small ? phi : qhi;
+    const V16 e{{static_cast<uint32_t>(olo), static_cast<uint32_t>(olo >> 32),
+                 static_cast<uint32_t>(ohi), static_cast<uint32_t>(ohi >> 32)}};
+    return off < 16 ? e : v;
 }
 CDB_HD uint32_t rest_distance(uint32_t off) {  // off * ceil(16 / off) for off < 16
-    return off >= 16 ? off : off * ((16 + off - 1) / off);
+    // Q - 16 for off = 1..15, one nibble each
+    return off < 16 ? 16 + static_cast<uint32_t>((0xECA8642052402000ull >> (4 * (off & 15))) & 15)
+                    : off;
 }
 
 // ---------------------------------------------------------------------------
@@ -455,8 +625,33 @@ struct Chunk {
     uint8_t* dst;
     uint64_t cap;
     uint64_t limit;    // LZ4: capacity; Snappy: declared length
+    long long tl = 0;  // profiling builds: thread 0's last phase mark
 
     CDB_HD Reader reader() const { return Reader{g, s.in, s.ibase}; }
+    // The staged bytes from the tile entry on, and how many of them the fast
+    // forms may read (also bounded by the chunk's end).
+    CDB_HD const uint8_t* staged() const { return s.in + (s.e - s.ibase); }
+    CDB_HD uint32_t staged_lim() const {
+        const uint64_t avail = kInBytes - (s.e - s.ibase);
+        const uint64_t rest = S > s.e ? S - s.e : 0;
+        return static_cast<uint32_t>(rest < avail ? rest : avail);
+    }
+    // The exact next position of the chain token at P (or kStepEnd) and its
+    // output length: the fast form when it applies.
+    CDB_HD uint64_t next_of(const Reader& in, const uint8_t* b, uint32_t lim, uint64_t P,
+                            uint64_t* ol) const {
+        if (P >= S) return kStepEnd;
+        const uint64_t r = P - s.e;
+        if (r < lim) {
+            uint32_t o32 = 0;
+            const uint32_t nr = F::step_rel(b, static_cast<uint32_t>(r), lim, &o32);
+            if (nr != kSlowRel) {
+                *ol = o32;
+                return s.e + nr;
+            }
+        }
+        return F::step(in, S, P, 0, ol);
+    }
     CDB_HD Ring ring() const { return Ring{s.ring, dst, reinterpret_cast<uintptr_t>(dst)}; }
 
     // ---- 1. stage the tile's input
@@ -483,13 +678,19 @@ struct Chunk {
     CDB_HD void seg_exits() {
         const Reader in = reader();
         const uint64_t e = s.e;
+        const uint8_t* b = staged();
+        const uint32_t lim = staged_lim();
         each([&](uint32_t t) {
             const uint32_t lo = t * kSeg, hi = lo + kSeg;
             for (int j = kSeg - 1; j >= 0; --j) {
                 const uint32_t r = lo + static_cast<uint32_t>(j);
                 const uint64_t P = e + r;
                 uint32_t v;
-                if (P >= S) {
+                uint32_t o32 = 0;
+                const uint32_t fr = r < lim ? F::step_rel(b, r, lim, &o32) : kSlowRel;
+                if (fr != kSlowRel) {
+                    v = fr >= hi ? fr : s.u.p.ex[exi(fr)];
+                } else if (P >= S) {
                     v = kEndMark;
                 } else {
                     uint64_t ol = 0;
@@ -575,6 +776,7 @@ struct Chunk {
                     P = cx == kEndMark ? kStepEnd : e + cx;
                 } else {
                     s.chosen[w] = kChoseOvr;
+                    LZC_EVENT(5, 1);
                     P = exact_walk(w, P);
                 }
             }
@@ -646,6 +848,8 @@ struct Chunk {
     CDB_HD void count() {
         const Reader in = reader();
         const uint64_t e = s.e;
+        const uint8_t* b = staged();
+        const uint32_t lim = staged_lim();
         each([&](uint32_t t) {
             const uint8_t c = entry_code(t);
             uint32_t n = 0;
@@ -658,7 +862,7 @@ struct Chunk {
                 while (P < hi) {
                     ++n;
                     uint64_t ol = 0;
-                    const uint64_t nx = P >= S ? kStepEnd : F::step(in, S, P, 0, &ol);
+                    const uint64_t nx = next_of(in, b, lim, P, &ol);
                     ol_sum += ol;
                     if (nx == kStepEnd) break;
                     P = nx;
@@ -686,6 +890,8 @@ struct Chunk {
     CDB_HD void check() {
         const Reader in = reader();
         const uint64_t e = s.e, d0 = s.d0;
+        const uint8_t* b = staged();
+        const uint32_t lim = staged_lim();
         each([&](uint32_t t) {
             if (t == 0) s.first_ev = 0xFFFFFFFFu;
         });
@@ -702,9 +908,18 @@ struct Chunk {
                     break;
                 }
                 lzl::Seq sq;
-                const int st = ladder_at(P, d0 + o, &sq);
-                uint64_t ol = 0;
-                const uint64_t nx = P >= S ? kStepEnd : F::step(in, S, P, 0, &ol);
+                int st = CUDEC_OK;
+                uint64_t nx, ol;
+                const uint64_t r = P - e;
+                if (r < lim && F::accept_rel(b, static_cast<uint32_t>(r), lim, P, d0 + o, limit,
+                                             &sq)) {
+                    nx = sq.next;
+                    ol = sq.lit + sq.ml;
+                } else {
+                    st = ladder_at(P, d0 + o, &sq);
+                    ol = 0;
+                    nx = next_of(in, b, lim, P, &ol);
+                }
                 s.u.t.pos[i] = static_cast<uint32_t>(P - e);
                 s.u.t.lit[i] = sq.lit > 0xFFFFFFFFull ? 0xFFFFFFFFu : static_cast<uint32_t>(sq.lit);
                 s.u.t.ml[i] = sq.ml > 0xFFFFFFFFull ? 0xFFFFFFFFu : static_cast<uint32_t>(sq.ml);
@@ -812,7 +1027,7 @@ struct Chunk {
             uint32_t m = ~0u;
             if (w == a >> 5) m &= ~0u << (a & 31);
             if (w == (b - 1) >> 5) m &= ~0u >> (31 - ((b - 1) & 31));
-            if (s.pend_bits[w] & m) return false;
+            if (*static_cast<volatile uint32_t*>(&s.pend_bits[w]) & m) return false;
         }
         return true;
     }
@@ -824,6 +1039,26 @@ struct Chunk {
             if (set) at_or(&s.pend_bits[w], m);
             else at_and(&s.pend_bits[w], ~m);
         }
+    }
+
+    // Token i's match if its source is ready: copied, then published.
+    CDB_HD bool try_match(const Ring& rg, uint32_t i, uint64_t G0) {
+        // the in-group part of its source, packed at the literal phase
+        const uint32_t dep = s.u.t.pos[i];
+        const uint32_t lo = dep & 0xFFFFu, hi = dep >> 16;
+        if (lo < hi && !bits_clear(lo, hi)) return false;
+        const uint32_t lit = s.u.t.lit[i], ml = s.u.t.ml[i], off = s.u.t.off[i];
+        const uint64_t ms = s.d0 + s.u.t.out[i] + lit;
+#if defined(__CUDA_ARCH__)
+        __threadfence_block();  // the source bytes' writers published before their bits cleared
+#endif
+        copy_match_ring(rg, ms, ml, off);
+#if defined(__CUDA_ARCH__)
+        __threadfence_block();  // the bytes land before the bits that publish them
+#endif
+        const uint32_t a = static_cast<uint32_t>(ms - G0);
+        bits_set(a, a + ml, false);
+        return true;
     }
 
     // Tokens [g0, g1), all of at most kBig bytes, output [G0, G1) within
@@ -871,57 +1106,73 @@ struct Chunk {
                     const uint32_t a = static_cast<uint32_t>(o + lit - G0);
                     bits_set(a, a + ml, true);
                     pm |= static_cast<uint8_t>(1u << k);
+                    // the part of its source inside the group, [lo, hi)
+                    // relative to G0 (empty: every source byte precedes the
+                    // group); the token's position is not needed past here
+                    const uint64_t ms = o + lit, src = ms - s.u.t.off[i];
+                    const uint64_t lo = src > G0 ? src : G0;
+                    const uint64_t hi = src + ml < ms ? src + ml : ms;
+                    s.u.t.pos[i] = lo < hi ? static_cast<uint32_t>(lo - G0) |
+                                                 (static_cast<uint32_t>(hi - G0) << 16)
+                                           : 0u;
                 }
             }
             s.pend[t] = pm;
         });
-        // matches, in rounds
-        uint32_t rounds = 0;
-        bool any = true;
-        while (any) {
-            each([&](uint32_t t) {
-                uint8_t dn = 0;
-                const uint8_t pm = s.pend[t];
-                for (uint32_t k = 0; k < kPerThread; ++k) {
-                    if (!(pm & (1u << k))) continue;
-                    const uint32_t i = g0 + t + k * kThreads;
-                    const uint32_t lit = s.u.t.lit[i], ml = s.u.t.ml[i], off = s.u.t.off[i];
-                    const uint64_t ms = d0 + s.u.t.out[i] + lit;
-                    const uint64_t src = ms - off;
-                    const uint64_t lo = src > G0 ? src : G0;
-                    const uint64_t hi = src + ml < ms ? src + ml : ms;
-                    const bool ready = lo >= hi || bits_clear(static_cast<uint32_t>(lo - G0),
-                                                              static_cast<uint32_t>(hi - G0));
-                    if (ready) {
-                        copy_match_ring(rg, ms, ml, off);
-                        dn |= static_cast<uint8_t>(1u << k);
+        LZC_PHASE(6);
+        LZC_EVENT(3, 1);
+        // matches, as data flow: every thread copies each of its pending
+        // matches once no byte its source reads is still pending, then
+        // publishes it (block fence, then its pending bits cleared). The
+        // lowest pending match of the group is always ready, so every pass
+        // over the CTA makes progress; passes per thread are bounded.
+#if defined(__CUDA_ARCH__)
+        each([&](uint32_t t) {
+            uint8_t pm = s.pend[t];
+            uint32_t spin = 0;
+            for (; pm; ++spin) {
+                // a thread's matches in order (its lowest pending first): a
+                // warp's lanes then hold consecutive tokens and copy together
+                for (uint32_t k = 0; k < kPerThread; ++k)
+                    if (pm & (1u << k)) {
+                        if (try_match(rg, g0 + t + k * kThreads, G0))
+                            pm = static_cast<uint8_t>(pm & ~(1u << k));
+                        break;
                     }
+                if (pm && spin >= kSpinCap) {  // unreachable: see above
+                    atomicExch(reinterpret_cast<int*>(&s.status), CUDEC_ERR_CUDA);
+                    break;
                 }
-                s.done[t] = dn;
-            });
-            any = each_or([&](uint32_t t) {
-                const uint8_t dn = s.done[t];
-                for (uint32_t k = 0; k < kPerThread; ++k) {
-                    if (!(dn & (1u << k))) continue;
-                    const uint32_t i = g0 + t + k * kThreads;
-                    const uint64_t ms = d0 + s.u.t.out[i] + s.u.t.lit[i];
-                    const uint32_t a = static_cast<uint32_t>(ms - G0);
-                    bits_set(a, a + s.u.t.ml[i], false);
-                }
-                s.pend[t] = static_cast<uint8_t>(s.pend[t] & ~dn);
-                return s.pend[t] != 0;
-            });
-            if (++rounds > g1 - g0 + 1) {  // unreachable: every round finishes a match
-                each([&](uint32_t t) {
-                    if (t == 0) s.status = CUDEC_ERR_CUDA;
-                });
-                return;
+            }
+#ifdef CDB_PHASE_TIMING
+            atomicAdd(&lzc_events[6], static_cast<unsigned long long>(spin));
+#endif
+        });
+#else
+        for (uint32_t pass = 0;; ++pass) {
+            bool any = false;
+            for (uint32_t t = 0; t < kThreads; ++t) {
+                uint8_t pm = s.pend[t];
+                for (uint32_t k = 0; k < kPerThread; ++k)
+                    if ((pm & (1u << k)) && try_match(rg, g0 + t + k * kThreads, G0))
+                        pm = static_cast<uint8_t>(pm & ~(1u << k));
+                s.pend[t] = pm;
+                any = any || pm != 0;
+            }
+            if (!any) break;
+            if (pass > g1 - g0) {  // unreachable: every pass finishes a match
+                s.status = CUDEC_ERR_CUDA;
+                break;
             }
         }
+#endif
+        LZC_EVENT(2, 1);
+        LZC_PHASE(7);
         flush(G1, false);
         each([&](uint32_t t) {
             if (t == 0) s.dend = G1;
         });
+        LZC_PHASE(8);
     }
 
     // One token longer than kBig: the whole CTA copies it straight to the
@@ -985,6 +1236,8 @@ struct Chunk {
                 s.dend = end;
             }
         });
+        LZC_PHASE(9);
+        LZC_EVENT(4, 1);
     }
 
     CDB_HD void execute(uint32_t ne) {
@@ -1008,6 +1261,7 @@ struct Chunk {
                 }
             });
             const uint32_t c = s.cut;
+            LZC_PHASE(10);
             if (c == g0) {
                 exec_big(g0);
                 g0 += 1;
@@ -1038,14 +1292,23 @@ struct Chunk {
         // every tile holds at least one token and consumes at least one
         // position, so the chunk's tiles number at most S + 1
         uint64_t fuel = S == ~0ull ? ~0ull : S + 1;
+        LZC_START();
         for (;;) {
             stage();
+            LZC_PHASE(0);
             seg_exits();
+            LZC_PHASE(1);
             cand_chase();
+            LZC_PHASE(2);
             tile_chase();
+            LZC_PHASE(3);
             count();
+            LZC_PHASE(4);
             if (s.ntok > F::kMaxTok) return CUDEC_ERR_CUDA;  // unreachable (tile bounds)
             check();
+            LZC_PHASE(5);
+            LZC_EVENT(0, 1);
+            LZC_EVENT(1, s.ntok);
             const uint32_t fe = s.first_ev;
 #ifdef LZC_TRACE
             LZC_TRACE(s.e, s.d0, s.ntok, s.ototal, fe, s.ev_kind, s.ev_status, s.tile_exit);
@@ -1079,7 +1342,7 @@ struct Chunk {
 // the batch. Dynamic shared memory: sizeof(Shm<F>).
 #if defined(__CUDACC__)
 template <class F>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, kCtasPerSm)
     lz_cta_kernel(const void* const* src_ptrs, const size_t* src_sizes, void* const* dst_ptrs,
                   const size_t* dst_caps, size_t n, cudec_chunk_result* results) {
     extern __shared__ __align__(16) uint8_t lzc_smem[];

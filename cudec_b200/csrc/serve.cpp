@@ -414,15 +414,28 @@ cudec_status cudec_server_submit(cudec_server* server, const void* h_input, size
     return CUDEC_OK;
 }
 
-cudec_status cudec_server_wait(cudec_server* server, uint64_t ticket,
-                               cudec_chunk_result* h_results, void** h_dst_ptrs,
-                               double* out_latency_ms) {
-    if (server == nullptr) return CUDEC_ERR_INVALID_ARGUMENT;
+}  // extern "C"
+
+namespace {
+
+// The wait of both entries; timeout_ms < 0 waits for good. *done = whether
+// the request completed within the time (nothing is written otherwise).
+cudec_status wait_request(cudec_server* server, uint64_t ticket, double timeout_ms, int* done,
+                          cudec_chunk_result* h_results, void** h_dst_ptrs,
+                          double* out_latency_ms) {
     std::unique_lock<std::mutex> lk(server->mu);
     auto it = server->reqs.find(ticket);
     if (it == server->reqs.end()) return CUDEC_ERR_INVALID_ARGUMENT;
     Request& r = *it->second;
-    server->cv.wait(lk, [&] { return r.state == Request::kDone; });
+    const auto finished = [&] { return r.state == Request::kDone; };
+    if (timeout_ms < 0) {
+        server->cv.wait(lk, finished);
+    } else if (!server->cv.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms),
+                                    finished)) {
+        *done = 0;
+        return CUDEC_OK;
+    }
+    *done = 1;
     if (h_results) std::memcpy(h_results, r.results.data(), r.n * sizeof(cudec_chunk_result));
     if (h_dst_ptrs) {
         uint8_t* out = static_cast<uint8_t*>(server->arena_base) + r.block +
@@ -433,6 +446,28 @@ cudec_status cudec_server_wait(cudec_server* server, uint64_t ticket,
         *out_latency_ms =
             std::chrono::duration<double, std::milli>(r.t_done - r.t_submit).count();
     return r.status;
+}
+
+}  // namespace
+
+extern "C" {
+
+cudec_status cudec_server_wait(cudec_server* server, uint64_t ticket,
+                               cudec_chunk_result* h_results, void** h_dst_ptrs,
+                               double* out_latency_ms) {
+    if (server == nullptr) return CUDEC_ERR_INVALID_ARGUMENT;
+    int done = 0;
+    return wait_request(server, ticket, -1.0, &done, h_results, h_dst_ptrs, out_latency_ms);
+}
+
+cudec_status cudec_server_wait_for(cudec_server* server, uint64_t ticket, double timeout_ms,
+                                   int* out_done, cudec_chunk_result* h_results,
+                                   void** h_dst_ptrs, double* out_latency_ms) {
+    if (server == nullptr || out_done == nullptr || !(timeout_ms >= 0.0))
+        return CUDEC_ERR_INVALID_ARGUMENT;
+    *out_done = 0;
+    return wait_request(server, ticket, timeout_ms, out_done, h_results, h_dst_ptrs,
+                        out_latency_ms);
 }
 
 cudec_status cudec_server_release(cudec_server* server, uint64_t ticket) {

@@ -283,6 +283,16 @@ cudec_status cudec_server_wait(cudec_server* server, uint64_t ticket,
                                cudec_chunk_result* h_results, void** h_dst_ptrs,
                                double* out_latency_ms);
 
+/* The same with a deadline: waits at most timeout_ms (>= 0) milliseconds.
+ * If the request completed, *out_done = 1 and the outputs are as for
+ * cudec_server_wait; otherwise *out_done = 0, CUDEC_OK is returned and
+ * nothing else is written (wait again later). A negative or NaN timeout or a
+ * NULL out_done is CUDEC_ERR_INVALID_ARGUMENT. No counterpart in the
+ * reference. */
+cudec_status cudec_server_wait_for(cudec_server* server, uint64_t ticket, double timeout_ms,
+                                   int* out_done, cudec_chunk_result* h_results,
+                                   void** h_dst_ptrs, double* out_latency_ms);
+
 /* Returns the request's device memory to the budget (after wait). */
 cudec_status cudec_server_release(cudec_server* server, uint64_t ticket);
 

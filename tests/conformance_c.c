@@ -158,6 +158,11 @@ int main(void) {
         CHECK(cudec_server_submit(0, storage, 8, offs, sizes, caps, formats, 1, &ticket) ==
               CUDEC_ERR_INVALID_ARGUMENT);
         CHECK(cudec_server_wait(0, 1, 0, 0, &ms) == CUDEC_ERR_INVALID_ARGUMENT);
+        {
+            int done = 7;
+            CHECK(cudec_server_wait_for(0, 1, 5.0, &done, 0, 0, &ms) ==
+                  CUDEC_ERR_INVALID_ARGUMENT);
+        }
         CHECK(cudec_server_release(0, 1) == CUDEC_ERR_INVALID_ARGUMENT);
         CHECK(cudec_server_destroy(0) == CUDEC_ERR_INVALID_ARGUMENT);
     }

@@ -128,5 +128,8 @@ def test_server_rejects_without_cuda():
     assert cd.lib().cudec_server_submit(None, a, 8, a, a, a, a, 1, ctypes.byref(t)) == \
         cd.ERR_INVALID_ARGUMENT
     assert cd.lib().cudec_server_wait(None, 1, None, None, None) == cd.ERR_INVALID_ARGUMENT
+    done = ctypes.c_int(7)
+    assert cd.lib().cudec_server_wait_for(None, 1, 5.0, ctypes.byref(done), None, None,
+                                          None) == cd.ERR_INVALID_ARGUMENT
     assert cd.lib().cudec_server_release(None, 1) == cd.ERR_INVALID_ARGUMENT
     assert cd.lib().cudec_server_destroy(None) == cd.ERR_INVALID_ARGUMENT

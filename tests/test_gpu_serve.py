@@ -2,6 +2,7 @@
 decoded while others are in flight give exactly the records and bytes they
 give alone, and both equal the oracle; the device-memory budget admits
 requests only when they fit; the plain (per-format, one slot) path agrees."""
+import ctypes
 import threading
 import random
 import time
@@ -118,3 +119,36 @@ def test_plain_mode_agrees(cuda):
         assert x == y and xo == yo
     a.close()
     b.close()
+
+
+def test_bounded_wait(cuda):
+    """cudec_server_wait_for: a deadline that passes first reports not done
+    and writes nothing; a later bounded wait returns the request's records,
+    which equal the oracle's; bad arguments are refused."""
+    import numpy as np
+    reqs = make_requests(3, 11)
+    srv = cd.Server(512 << 20, max_inflight=1)
+    tickets = []
+    for r in reqs:
+        st, t = srv.submit(r["packed"], r["offs"], r["sizes"], r["caps"], r["fmts"])
+        assert st == 0
+        tickets.append(t)
+    for r, t in zip(reqs, tickets):
+        st, done, recs, ptrs, lat = srv.wait_for(t, 0.0)
+        assert st == 0
+        if not done:  # nothing written on a missed deadline
+            assert (recs["status"] == 0).all() and (recs["bytes_written"] == 0).all()
+            assert (ptrs == 0).all()
+        st, done, recs, ptrs, lat = srv.wait_for(t, 120000.0)
+        assert st == 0 and done and lat >= 0
+        for i, (c, cap, f) in enumerate(zip(r["comps"], r["caps"], r["fmts"])):
+            ost, oout = ORACLE[f](c, cap)
+            assert (int(recs[i]["status"]), int(recs[i]["bytes_written"])) == \
+                (ost, len(oout) if ost == 0 else 0), (i, f)
+        assert srv.release(t) == 0
+    done = ctypes.c_int(0)
+    assert cd.lib().cudec_server_wait_for(srv.handle, 12345, 1.0, ctypes.byref(done), None,
+                                          None, None) == cd.ERR_INVALID_ARGUMENT
+    assert cd.lib().cudec_server_wait_for(srv.handle, 1, -1.0, ctypes.byref(done), None,
+                                          None, None) == cd.ERR_INVALID_ARGUMENT
+    srv.close()
