@@ -43,7 +43,7 @@ the launch itself is bracketed by CUDA events on its stream.
             32 GiB device budget, outputs kept on the device; p50 /
             p99 latency and aggregate GB/s of the continuous-batching server
             against the plain path (one request at a time, one launch per
-            format)
+            format), at the default rate and at the `--serve-sweep` rates
   per_format    the same measurement for raw Snappy (same content) and for
             Zstd: 4,096 frames of 1 MiB (1 MiB window, 128 KiB blocks, 10%
             repeated-byte runs, back-references up to 1 MiB), libzstd level 3
@@ -97,6 +97,9 @@ def parse_args():
                     help="requests of the served mixed-format stream (0 skips it)")
     ap.add_argument("--serve-rate", type=float, default=200.0,
                     help="Poisson arrival rate of the served stream (requests/s)")
+    ap.add_argument("--serve-sweep", default="25,50,100",
+                    help="further arrival rates (requests/s, comma-separated) replayed "
+                         "for the latency sweep, below the saturating default rate")
     ap.add_argument("--gdeflate-streams", type=int, default=16384,
                     help="256 KiB TileStreams of the GDeflate leg (0 skips it)")
     ap.add_argument("--gdeflate-unique", type=int, default=0,
@@ -354,10 +357,10 @@ def run_mixed(torch, cd, DeviceBatch, args, dev, stream, flush, max_over_ranks, 
     in_bytes = int(sum(len(c) for c in comps))
     allb = DeviceBatch(comps, caps, device=dev, poison=None)
     plan = cd.MixedPlan()
-    s = stream.cuda_stream
+    default_shape = plan.shape()  # compiled in: the same on every run
     with torch.cuda.stream(stream):
-        assert allb.run_mixed(plan, fmts, stream, tune=True) == 0
-    tuning = plan.tuning()
+        assert allb.run_mixed(plan, fmts, stream) == 0
+    stream.synchronize()
     res = allb.results()
     assert (res["status"] == 0).all() and (res["bytes_written"] == np.array(caps)).all()
     steps = max(args.steps // 50, 3)
@@ -366,6 +369,15 @@ def run_mixed(torch, cd, DeviceBatch, args, dev, stream, flush, max_over_ranks, 
     res = allb.results()
     assert (res["status"] == 0).all() and (res["bytes_written"] == np.array(caps)).all()
     verified = verify_outputs(allb, caps, expect=raws)
+    # the autotuner's shape for this batch, measured the same way
+    with torch.cuda.stream(stream):
+        assert allb.run_mixed(plan, fmts, stream, tune=True) == 0
+    tuned_shape = plan.shape()
+    t_ms = max_over_ranks(time_region(torch, stream, flush, steps, warm,
+                                      lambda: allb.run_mixed(plan, fmts, stream)))
+    res = allb.results()
+    assert (res["status"] == 0).all() and (res["bytes_written"] == np.array(caps)).all()
+    assert verify_outputs(allb, caps, expect=raws) == n
     plan.close()
     del allb
     torch.cuda.empty_cache()
@@ -396,8 +408,15 @@ def run_mixed(torch, cd, DeviceBatch, args, dev, stream, flush, max_over_ranks, 
         "decompressed_bytes": out_bytes, "compressed_bytes": in_bytes,
         "largest_chunk": int(sizes.max()), "median_chunk": int(np.median(sizes)),
         "roofline_frac": round((in_bytes + out_bytes) / (p_ms * 1e-3) / 1e9 / peaks()[0], 5),
-        "tuning_per_bucket": [list(t) for t in tuning],
-        "path": "cudec_mixed_decompress (graph: order + persistent work-stealing kernel) vs "
+        "shape_per_bucket": [list(t) for t in default_shape],
+        "shape_source": "compiled-in default (warps per LZ4/Snappy chunk, then the one-warp "
+                        "parse reach, lookahead, ring batch; buckets <4K,<16K,<64K,<256K,<1M,"
+                        "larger)",
+        "tuned": {"value": round(world * out_bytes / (t_ms * 1e-3) / 1e9, 3),
+                  "ms_per_step": round(t_ms, 3),
+                  "shape_per_bucket": [list(t) for t in tuned_shape]},
+        "path": "cudec_mixed_decompress (graph: order + persistent work-stealing warp grid beside "
+                "a CTA-per-chunk grid) vs "
                 "cudec_lz4_decompress_batch + cudec_snappy_decompress_batch",
     }
 
@@ -535,7 +554,15 @@ def run_serve(cd, args, dev):
     total = float(sum(sum(r["caps"]) for r in reqs))
     mixed = serve_once(cd, reqs, cd.SERVER_MIXED, SERVE_SLOTS, args.serve_rate)
     plain = serve_once(cd, reqs, cd.SERVER_PLAIN, 1, args.serve_rate)
-    return {"continuous_batching": mixed, "plain_queue": plain,
+    sweep = []
+    for rate in [float(r) for r in args.serve_sweep.split(",") if r]:
+        m = serve_once(cd, reqs, cd.SERVER_MIXED, SERVE_SLOTS, rate)
+        q = serve_once(cd, reqs, cd.SERVER_PLAIN, 1, rate)
+        sweep.append({"rate_per_s": rate,
+                      "offered_GBps": round(total / len(reqs) * rate / 1e9, 3),
+                      "continuous_batching": {k: m[k] for k in ("p50_ms", "p99_ms", "value")},
+                      "plain_queue": {k: q[k] for k in ("p50_ms", "p99_ms", "value")}})
+    return {"continuous_batching": mixed, "plain_queue": plain, "sweep": sweep,
             "requests": len(reqs), "rate_per_s": args.serve_rate,
             "chunks": int(sum(len(r["caps"]) for r in reqs)),
             "decompressed_bytes": int(total),

@@ -63,6 +63,8 @@ SIGNATURES = {
     "cudec_mixed_decompress": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _SZ, _P, _P]),
     "cudec_mixed_plan_tune": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _SZ, _P, _P]),
     "cudec_mixed_plan_get_tuning": (ctypes.c_int, [_P, _P]),
+    "cudec_mixed_plan_get_shape": (ctypes.c_int, [_P, _P]),
+    "cudec_mixed_plan_set_shape": (ctypes.c_int, [_P, _P]),
     "cudec_server_create": (ctypes.c_int, [_SZ, ctypes.c_int, ctypes.c_int, _SZ, _P]),
     "cudec_server_destroy": (ctypes.c_int, [_P]),
     "cudec_server_submit": (ctypes.c_int, [_P, _P, _SZ, _P, _P, _P, _P, _SZ, _P]),
@@ -253,6 +255,20 @@ class MixedPlan:
         if st != OK:
             raise RuntimeError("cudec_mixed_plan_get_tuning: %s" % STATUS_NAMES.get(st, st))
         return [tuple(out[3 * b:3 * b + 3]) for b in range(MIXED_BUCKETS)]
+
+    def shape(self):
+        """[(warps per chunk, parse reach, lookahead, ring batch)] per bucket."""
+        out = (ctypes.c_uint32 * (4 * MIXED_BUCKETS))()
+        st = lib().cudec_mixed_plan_get_shape(self.handle, out)
+        if st != OK:
+            raise RuntimeError("cudec_mixed_plan_get_shape: %s" % STATUS_NAMES.get(st, st))
+        return [tuple(out[4 * b:4 * b + 4]) for b in range(MIXED_BUCKETS)]
+
+    def set_shape(self, shape):
+        """Set [(warps, reach, lookahead, batch)] per bucket; returns the status."""
+        flat = [int(v) for row in shape for v in row]
+        arr = (ctypes.c_uint32 * len(flat))(*flat)
+        return lib().cudec_mixed_plan_set_shape(self.handle, arr)
 
     def close(self):
         if self.handle:

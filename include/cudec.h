@@ -231,8 +231,10 @@ cudec_status cudec_mixed_decompress(cudec_mixed_plan* plan,
 
 /* Autotuner: decodes the given batch once per candidate shape (parse reach,
  * input lookahead, ring batch), bucket by bucket, timing each on the device,
- * and keeps the fastest per bucket. Synchronous; destinations and results
- * receive the normal decode. */
+ * and keeps the fastest per bucket; then, per bucket, times its LZ4 and
+ * Snappy chunks under that one-warp shape against a whole CTA per chunk and
+ * keeps the faster. Synchronous; destinations and results receive the
+ * normal decode. */
 cudec_status cudec_mixed_plan_tune(cudec_mixed_plan* plan,
                                    const void* const* d_src_ptrs,
                                    const size_t* d_src_sizes,
@@ -246,6 +248,18 @@ cudec_status cudec_mixed_plan_tune(cudec_mixed_plan* plan,
 /* out_params[3*b .. 3*b+2] = parse reach, lookahead, ring batch of bucket b. */
 cudec_status cudec_mixed_plan_get_tuning(const cudec_mixed_plan* plan,
                                          uint32_t* out_params);
+
+/* The whole decode shape, 4 values per bucket b: out_shape[4*b] = warps per
+ * LZ4 / Snappy chunk (1: one warp; 8: a whole CTA runs the CTA-per-chunk
+ * decoder), then parse reach, lookahead and ring batch of the one-warp
+ * decoder. A plan starts from a compiled-in table (a CTA per chunk from
+ * 64 KiB of output up); cudec_mixed_plan_tune measures one on the caller's
+ * chunks. A caller can save the shape and set it on later plans, so the
+ * decode shape is fixed across runs; set_shape refuses (INVALID_ARGUMENT,
+ * nothing changed) a warps value other than 1 or 8 or an out-of-range
+ * one-warp shape. Any shape decodes identically; it only moves time. */
+cudec_status cudec_mixed_plan_get_shape(const cudec_mixed_plan* plan, uint32_t* out_shape);
+cudec_status cudec_mixed_plan_set_shape(cudec_mixed_plan* plan, const uint32_t* shape);
 
 /* ---------------------------------------------------------------------
  * Continuous-batching decode server (no counterpart in the reference). A

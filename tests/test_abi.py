@@ -112,6 +112,8 @@ def test_mixed_plan_rejects_without_cuda():
     assert m(None, a, a, a, a, a, 4, a, None) == cd.ERR_INVALID_ARGUMENT
     assert cd.lib().cudec_mixed_plan_tune(None, a, a, a, a, a, 4, a, None) == cd.ERR_INVALID_ARGUMENT
     assert cd.lib().cudec_mixed_plan_get_tuning(None, a) == cd.ERR_INVALID_ARGUMENT
+    assert cd.lib().cudec_mixed_plan_get_shape(None, a) == cd.ERR_INVALID_ARGUMENT
+    assert cd.lib().cudec_mixed_plan_set_shape(None, a) == cd.ERR_INVALID_ARGUMENT
 
 
 def test_server_rejects_without_cuda():

@@ -116,6 +116,37 @@ def test_new_arguments_recapture_and_unknown_codes(cuda):
     plan.close()
 
 
+def test_warps_per_chunk_shapes_agree(cuda):
+    """Every LZ4 / Snappy chunk on one warp, every one on a whole CTA (the
+    CTA-per-chunk decoder beside the warp grid), and the compiled-in default:
+    identical records and bytes, equal to the per-format entries. Shapes
+    read back as set; invalid shapes are refused and change nothing."""
+    import torch
+    from cudec_b200.device import DeviceBatch
+    raws, comps, caps, fmts = make_batch(500, 41, hi=2 << 20)
+    recs, outs = per_format(cuda, comps, caps, fmts)
+    plan = cd.MixedPlan()
+    default = plan.shape()
+    assert [s[0] for s in default] == [1, 1, 1, 8, 8, 8]
+    b = DeviceBatch(comps, caps, device=cuda)
+    for wpc in (1, 8, None):
+        shape = default if wpc is None else [(wpc,) + tuple(s[1:]) for s in default]
+        assert plan.set_shape(shape) == 0
+        assert plan.shape() == [tuple(s) for s in shape]
+        b.reset()
+        assert b.run_mixed(plan, fmts) == 0
+        torch.cuda.synchronize()
+        check(b, recs, outs, "warps per chunk %s" % wpc)
+    bad = [list(s) for s in default]
+    bad[2][0] = 4
+    assert plan.set_shape(bad) == cd.ERR_INVALID_ARGUMENT
+    bad = [list(s) for s in default]
+    bad[0][1] = 7
+    assert plan.set_shape(bad) == cd.ERR_INVALID_ARGUMENT
+    assert plan.shape() == [tuple(s) for s in default]
+    plan.close()
+
+
 def test_tuner_keeps_results_and_reports_valid_shapes(cuda):
     import torch
     from cudec_b200.device import DeviceBatch
@@ -127,6 +158,7 @@ def test_tuner_keeps_results_and_reports_valid_shapes(cuda):
     check(b, recs, outs, "tuning run")
     for pw, ahead, batch in plan.tuning():
         assert pw in (256, 512, 1024) and pw + 64 <= ahead <= 4032 and batch in (2048, 4096)
+    assert all(s[0] in (1, 8) for s in plan.shape())
     b.reset()
     assert b.run_mixed(plan, fmts) == 0
     torch.cuda.synchronize()
