@@ -810,6 +810,50 @@ def main():
 
     e2e_staged_ms = e2e_ms_for(staged_ptrs_h)
     e2e_ms = e2e_ms_for(src_ptrs_h)
+
+    # host output: the same call with every destination in pinned host
+    # memory (the decoded bytes are copied back inside the call)
+    host_out = torch.empty(out_bytes, dtype=torch.uint8).pin_memory()
+    host_dst_h = (np.arange(n, dtype=np.uint64) * np.uint64(CHUNK) +
+                  np.uint64(host_out.data_ptr())).astype(np.uint64)
+    ctx = cd.StreamContext()
+    ho_times = []
+    for k in range(warm + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        rc = ctx.decode(src_ptrs_h.ctypes.data, sizes_h.ctypes.data, host_dst_h.ctypes.data,
+                        caps_h.ctypes.data, n, cd.MEM_HOST, res_h.ctypes.data)
+        t1 = time.perf_counter()
+        assert rc == 0 and (res_h["s"] == 0).all()
+        if k >= warm:
+            ho_times.append(t1 - t0)
+    ctx.close()
+    hnp = host_out.numpy()
+    assert all(np.array_equal(hnp[CHUNK * i:CHUNK * (i + 1)], raws[i]) for i in range(n))
+    ho_ms = max_over_ranks(1e3 * sum(ho_times) / len(ho_times))
+
+    # the .lz4 frame entry, host to host: the whole batch's content as one
+    # frame of independent 4 MiB blocks with block and content checksums
+    from cudec_b200 import workload as W
+    content = np.concatenate(raws).tobytes()
+    frame = W.lz4f_compress(content, block_size_id=7, independent=True, content_checksum=True,
+                            block_checksum=True)
+    import ctypes
+    f_src = np.frombuffer(frame, dtype=np.uint8).copy()
+    f_out = np.empty(len(content), dtype=np.uint8)
+    f_written = ctypes.c_size_t(0)
+    f_times = []
+    for k in range(warm + max(args.steps // 4, 3)):
+        t0 = time.perf_counter()
+        st = cd.lib().cudec_lz4f_decompress(f_src.ctypes.data, len(frame), f_out.ctypes.data,
+                                            len(content), ctypes.byref(f_written))
+        t1 = time.perf_counter()
+        assert st == 0 and f_written.value == len(content)
+        if k >= warm:
+            f_times.append(t1 - t0)
+    assert f_out.tobytes() == content
+    f_ms = max_over_ranks(1e3 * sum(f_times) / len(f_times))
     e2e = world * out_bytes / (e2e_ms * 1e-3) / 1e9
     e2e_staged = world * out_bytes / (e2e_staged_ms * 1e-3) / 1e9
 
@@ -838,7 +882,19 @@ def main():
                     "ms_per_step": round(e2e_ms, 4),
                     "staged": {"value": round(e2e_staged, 3),
                                "ms_per_step": round(e2e_staged_ms, 4),
-                               "source": "pageable host chunks, copied up by the call"}},
+                               "source": "pageable host chunks, copied up by the call"},
+                    "host_out": {"value": round(world * out_bytes / (ho_ms * 1e-3) / 1e9, 3),
+                                 "ms_per_step": round(ho_ms, 4),
+                                 "d2h_bytes_per_step": out_bytes,
+                                 "dst": "pinned host memory, every decoded byte copied back "
+                                        "inside the call"},
+                    "frame": {"value": round(world * out_bytes / (f_ms * 1e-3) / 1e9, 3),
+                              "ms_per_step": round(f_ms, 4),
+                              "api": "cudec_lz4f_decompress, host frame -> host buffer",
+                              "frame": "the batch's 64 MiB as one .lz4 frame: independent "
+                                       "4 MiB blocks, block and content checksums (liblz4 "
+                                       "LZ4F_compressFrame)",
+                              "compressed_bytes": len(frame)}},
             "per_format": {
                 "lz4": {"value": round(value, 3), "ms_per_step": round(mean_ms, 5)},
                 "snappy": {"value": round(world * out_bytes / (s_ms * 1e-3) / 1e9, 3),

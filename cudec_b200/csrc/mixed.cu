@@ -256,9 +256,11 @@ __global__ void __launch_bounds__(kThreads, 2) mixed_kernel(Args a) {
 }
 
 // Warps per LZ4 / Snappy chunk by bucket when the plan is created: a whole
-// CTA from 64 KiB of output up (where the CTA decoder's parallel parse beats
-// one warp's serial chain), one warp below.
-constexpr uint32_t kDefaultWpc[kBuckets] = {1, 1, 1, kCtaWarps, kCtaWarps, kCtaWarps};
+// CTA in every bucket (measured on B200 over 100,000 uneven LZ4 + Snappy
+// chunks: the CTA decoder's parallel parse beats one warp's serial chain
+// from the smallest bucket up); Zstd and GDeflate chunks are one warp's.
+constexpr uint32_t kDefaultWpc[kBuckets] = {kCtaWarps, kCtaWarps, kCtaWarps,
+                                            kCtaWarps, kCtaWarps, kCtaWarps};
 
 struct Key {
     const void* const* src;
@@ -280,7 +282,7 @@ struct Key {
 struct cudec_mixed_plan {
     int dev = -1;
     unsigned grid = 0;      // warp grid: resident CTAs x SMs
-    unsigned cta_grid = 0;  // CTA grid: at most one CTA per SM
+    unsigned cta_grid = 0;  // CTA grid: resident CTAs x SMs
     int sms = 0;
     cdb::DevBuf ctrl, order, slots;
     cudaStream_t s = nullptr, s2 = nullptr;  // s2: the CTA grid beside the warp grid
@@ -453,7 +455,7 @@ cudec_status cudec_mixed_plan_create(cudec_mixed_plan** out_plan) {
                    &cta_per_sm, cdb::mixed::mixed_cta_kernel, cdb::lzc::kThreads,
                    cdb::mixed::kCtaSmem) == cudaSuccess;
     ok = ok && cta_per_sm > 0;
-    if (ok) p->cta_grid = static_cast<unsigned>(p->sms);  // leaves room for the warp grid
+    if (ok) p->cta_grid = static_cast<unsigned>(p->sms * cta_per_sm);
     ok = ok && p->ctrl.ensure(sizeof(Ctrl)) == cudaSuccess;
     ok = ok && p->slots.ensure(static_cast<size_t>(p->grid) * cdb::mixed::kWarps *
                                cdb::zstd::kLitSlot) == cudaSuccess;
