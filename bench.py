@@ -207,16 +207,22 @@ def peaks():
         return 6650.0, "fallback"
 
 
+TRAFFIC_PROFILE = os.path.join("profiles", "lz4_cta_kernel_64KiBx1024.txt")
+
+
 def traffic_per_launch():
-    """DRAM bytes per launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "lz4_batch_64KiBx1024.txt")
+    """(DRAM bytes, L2 write bytes, build) per headline launch from the
+    committed ncu summary (Nones where absent)."""
+    vals = {}
     try:
-        for line in open(path):
-            if line.startswith("dram_bytes_per_launch="):
-                return int(line.split("=", 1)[1].split()[0])
+        for line in open(os.path.join(ROOT, TRAFFIC_PROFILE)):
+            for key in ("dram_bytes_per_launch=", "l2_write_bytes_per_launch=", "build:"):
+                if line.startswith(key):
+                    vals[key] = line.split(key[-1], 1)[1].strip()
     except OSError:
         pass
-    return None
+    num = lambda k: int(vals[k].split()[0]) if k in vals else None
+    return num("dram_bytes_per_launch="), num("l2_write_bytes_per_launch="), vals.get("build:")
 
 
 class ClockSampler:
@@ -858,6 +864,7 @@ def main():
     e2e_staged = world * out_bytes / (e2e_staged_ms * 1e-3) / 1e9
 
     peak, peak_kind = peaks()
+    traffic = traffic_per_launch()
     achieved = (in_bytes + out_bytes) / (mean_ms * 1e-3) / 1e9
     if rank == 0:
         line = {
@@ -872,8 +879,10 @@ def main():
                        "l2": "flushed before every timed launch (256 MiB memset)"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 5),
-                         "traffic": traffic_per_launch(), "peak_source": peak_kind,
-                         "algorithmic_bytes_per_launch": in_bytes + out_bytes},
+                         "traffic": traffic[0], "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": in_bytes + out_bytes,
+                         "l2_write_bytes_per_launch": traffic[1],
+                         "traffic_source": "%s (%s)" % (TRAFFIC_PROFILE, traffic[2])},
             "e2e": {"value": round(e2e, 3), "unit": "GB/s",
                     "h2d_bytes_per_step": int(in_bytes + 32 * n),
                     "d2h_bytes_per_step": 16 * n,
