@@ -934,6 +934,12 @@ def main():
                                  "library": "liblz4 %d LZ4_decompress_safe"
                                             % oracle.oracle_lib().codec_lz4_version()}
             # the same measurement for the other formats' codec libraries
+            if oracle.ref_twin_lib() is not None:
+                rv, rused, rreps = cpu_sample("ref_snappy", scomps, caps, csec, threads)
+                line["per_format"]["snappy"]["cpu_baseline"] = {
+                    "value": round(rv, 3), "unit": "GB/s", "cores": rused, "kind": "reference",
+                    "sample": "%d passes over the %d x 64 KiB batch; reference twin "
+                              "tests/snappy_twin.h on a std::thread pool" % (rreps, n)}
             sv, sused, sreps = snappy_cpu(scomps, caps, csec, threads)
             line["per_format"]["snappy"]["cpu_codec"] = {
                 "value": round(sv, 3), "unit": "GB/s", "cores": sused,
