@@ -55,6 +55,7 @@ SIGNATURES = {
     "cudec_zstd_workspace_bytes": (ctypes.c_size_t, [_SZ]),
     "cudec_zstd_decompress_batch": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P, _SZ, _P]),
     "cudec_zstd_decompress_batch_noalloc": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P]),
+    "cudec_zstd_decompress_batch_multi": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P, _SZ, _P]),
     "cudec_gdeflate_decompress_batch": (ctypes.c_int, [_P, _P, _P, _P, _SZ, _P, _P]),
     "cudec_gdeflate_tilestream_parse": (ctypes.c_int, [_P, _SZ, _P, _SZ, _P, _P]),
     "cudec_gdeflate_tilestream_decompress": (ctypes.c_int, [_P, _SZ, _P, _SZ, ctypes.c_int, _P]),
@@ -131,6 +132,15 @@ def zstd_decompress_batch(d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_caps, n, d_
     """cudec_zstd_decompress_batch (one Zstd frame per chunk)."""
     return lib().cudec_zstd_decompress_batch(d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_caps,
                                              n, d_results, d_workspace, workspace_bytes, stream)
+
+
+def zstd_decompress_batch_multi(d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_caps, n, d_results,
+                                d_workspace, workspace_bytes, stream=None):
+    """cudec_zstd_decompress_batch_multi (a sequence of Zstd and skippable
+    frames per chunk, outputs concatenated)."""
+    return lib().cudec_zstd_decompress_batch_multi(d_src_ptrs, d_src_sizes, d_dst_ptrs,
+                                                   d_dst_caps, n, d_results, d_workspace,
+                                                   workspace_bytes, stream)
 
 
 ZSTD_NOALLOC_MAX_CHUNKS = 64

@@ -19,7 +19,7 @@ constexpr uint32_t kMaxSlots = 4096;  // frames decoded concurrently (workspace 
 __global__ void __launch_bounds__(kCtaThreads)
     zstd_decode_kernel(const void* const* src_ptrs, const size_t* src_sizes,
                        void* const* dst_ptrs, const size_t* dst_caps, size_t n,
-                       cudec_chunk_result* results, uint8_t* workspace) {
+                       cudec_chunk_result* results, uint8_t* workspace, bool multi = false) {
     __shared__ WarpSmem wsm[kWarpsPerCta];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const size_t gw = static_cast<size_t>(blockIdx.x) * kWarpsPerCta + warp;
@@ -27,9 +27,12 @@ __global__ void __launch_bounds__(kCtaThreads)
     uint8_t* litbuf = workspace + gw * kLitSlot;
     for (size_t c = gw; c < n; c += total) {
         uint64_t written = 0;
-        const int st = decode_frame(static_cast<const uint8_t*>(src_ptrs[c]), src_sizes[c],
-                                    static_cast<uint8_t*>(dst_ptrs[c]), dst_caps[c], wsm[warp],
-                                    litbuf, lane, &written);
+        const uint8_t* src = static_cast<const uint8_t*>(src_ptrs[c]);
+        uint8_t* dst = static_cast<uint8_t*>(dst_ptrs[c]);
+        const int st = multi ? decode_frames(src, src_sizes[c], dst, dst_caps[c], wsm[warp],
+                                             litbuf, lane, &written)
+                             : decode_frame(src, src_sizes[c], dst, dst_caps[c], wsm[warp],
+                                            litbuf, lane, &written);
         __syncwarp();
         if (lane == 0) {
             results[c].status = st;
@@ -51,14 +54,14 @@ size_t cudec_zstd_workspace_bytes(size_t chunk_count) {
     return rounded * cdb::zstd::kLitSlot;
 }
 
-cudec_status cudec_zstd_decompress_batch(const void* const* d_src_ptrs,
-                                         const size_t* d_src_sizes,
-                                         void* const* d_dst_ptrs,
-                                         const size_t* d_dst_capacities,
-                                         size_t chunk_count,
-                                         cudec_chunk_result* d_results,
-                                         void* d_workspace, size_t workspace_bytes,
-                                         cudec_stream_t stream) {
+}  // extern "C"
+
+namespace {
+
+cudec_status launch_zstd(const void* const* d_src_ptrs, const size_t* d_src_sizes,
+                         void* const* d_dst_ptrs, const size_t* d_dst_capacities,
+                         size_t chunk_count, cudec_chunk_result* d_results, void* d_workspace,
+                         size_t workspace_bytes, cudec_stream_t stream, bool multi) {
     const cudec_status v = cdb::validate_batch(d_src_ptrs, d_src_sizes, d_dst_ptrs,
                                                d_dst_capacities, chunk_count, d_results);
     if (v != CUDEC_OK) return v;
@@ -70,8 +73,36 @@ cudec_status cudec_zstd_decompress_batch(const void* const* d_src_ptrs,
     cdb::zstd::zstd_decode_kernel<<<grid, cdb::zstd::kCtaThreads, 0,
                                     reinterpret_cast<cudaStream_t>(stream)>>>(
         d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_capacities, chunk_count, d_results,
-        static_cast<uint8_t*>(d_workspace));
+        static_cast<uint8_t*>(d_workspace), multi);
     return cudaGetLastError() == cudaSuccess ? CUDEC_OK : CUDEC_ERR_CUDA;
+}
+
+}  // namespace
+
+extern "C" {
+
+cudec_status cudec_zstd_decompress_batch(const void* const* d_src_ptrs,
+                                         const size_t* d_src_sizes,
+                                         void* const* d_dst_ptrs,
+                                         const size_t* d_dst_capacities,
+                                         size_t chunk_count,
+                                         cudec_chunk_result* d_results,
+                                         void* d_workspace, size_t workspace_bytes,
+                                         cudec_stream_t stream) {
+    return launch_zstd(d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_capacities, chunk_count,
+                       d_results, d_workspace, workspace_bytes, stream, false);
+}
+
+cudec_status cudec_zstd_decompress_batch_multi(const void* const* d_src_ptrs,
+                                               const size_t* d_src_sizes,
+                                               void* const* d_dst_ptrs,
+                                               const size_t* d_dst_capacities,
+                                               size_t chunk_count,
+                                               cudec_chunk_result* d_results,
+                                               void* d_workspace, size_t workspace_bytes,
+                                               cudec_stream_t stream) {
+    return launch_zstd(d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_capacities, chunk_count,
+                       d_results, d_workspace, workspace_bytes, stream, true);
 }
 
 }  // extern "C"

@@ -149,10 +149,14 @@ __device__ __forceinline__ void lane_match(uint8_t* dst, uint64_t ms, uint64_t n
     }
 }
 
-// Decode one frame; every lane returns the same status and *written.
-__device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, uint64_t cap,
-                            WarpSmem& w, uint8_t* litbuf, uint32_t lane, uint64_t* written) {
+// Decode the frame at the start of f[0, N); every lane returns the same
+// status, *written and *consumed (the frame's bytes). Bytes after the frame
+// are not looked at.
+__device__ inline int decode_frame_part(const uint8_t* f, uint64_t N, uint8_t* dst, uint64_t cap,
+                                        WarpSmem& w, uint8_t* litbuf, uint32_t lane,
+                                        uint64_t* written, uint64_t* consumed) {
     *written = 0;
+    *consumed = 0;
     if (N < 4) return CUDEC_ERR_CORRUPT_INPUT;
     const uint32_t magic = static_cast<uint32_t>(rd_le(f, 4));
     if (magic != 0xFD2FB528u) {
@@ -573,7 +577,53 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
         if (h != static_cast<uint32_t>(rd_le(f + pos, 4))) return CUDEC_ERR_CORRUPT_INPUT;
         pos += 4;
     }
-    if (pos != N) return CUDEC_ERR_CORRUPT_INPUT;
+    *written = out;
+    *consumed = pos;
+    return CUDEC_OK;
+}
+
+// One frame per chunk, the reference's rule (src/zstd_frame.h:196-409):
+// bytes after the frame are CORRUPT_INPUT, a skippable frame UNSUPPORTED.
+__device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, uint64_t cap,
+                                   WarpSmem& w, uint8_t* litbuf, uint32_t lane,
+                                   uint64_t* written) {
+    uint64_t out = 0, used = 0;
+    *written = 0;
+    const int st = decode_frame_part(f, N, dst, cap, w, litbuf, lane, &out, &used);
+    if (st != CUDEC_OK) return st;
+    if (used != N) return CUDEC_ERR_CORRUPT_INPUT;
+    *written = out;
+    return CUDEC_OK;
+}
+
+// A chunk of concatenated frames, as libzstd's ZSTD_decompress reads a
+// buffer (the first rung of the reference's subset ladder,
+// docs/MASTERPLAN.md:1286-1289): skippable frames (magic 0x184D2A50-5F,
+// 4-byte size) are skipped, each Zstd frame (in the v1 subset above)
+// decodes after the previous one's output; fewer than 4 bytes left, or a
+// skippable frame running past the chunk, is CORRUPT_INPUT.
+__device__ inline int decode_frames(const uint8_t* f, uint64_t N, uint8_t* dst, uint64_t cap,
+                                    WarpSmem& w, uint8_t* litbuf, uint32_t lane,
+                                    uint64_t* written) {
+    *written = 0;
+    uint64_t pos = 0, out = 0;
+    while (pos < N) {
+        if (N - pos < 4) return CUDEC_ERR_CORRUPT_INPUT;
+        const uint32_t magic = static_cast<uint32_t>(rd_le(f + pos, 4));
+        if (magic >= 0x184D2A50u && magic <= 0x184D2A5Fu) {
+            if (N - pos < 8) return CUDEC_ERR_CORRUPT_INPUT;
+            const uint64_t sz = rd_le(f + pos + 4, 4);
+            if (sz > N - pos - 8) return CUDEC_ERR_CORRUPT_INPUT;
+            pos += 8 + sz;
+            continue;
+        }
+        uint64_t fo = 0, used = 0;
+        const int st = decode_frame_part(f + pos, N - pos, dst + out, cap - out, w, litbuf, lane,
+                                         &fo, &used);
+        if (st != CUDEC_OK) return st;
+        out += fo;
+        pos += used;
+    }
     *written = out;
     return CUDEC_OK;
 }

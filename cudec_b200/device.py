@@ -75,9 +75,10 @@ class DeviceBatch:
         """Launch the format's batch entry on `stream` (torch stream or None =
         current stream). Returns the synchronous status."""
         s = (stream or torch.cuda.current_stream(self.device)).cuda_stream
-        if fmt == "zstd":
+        if fmt in ("zstd", "zstd_multi"):
             ws = self.workspace()
-            return cd.zstd_decompress_batch(*self.args(), ws.data_ptr(), ws.numel(), s)
+            fn = cd.zstd_decompress_batch if fmt == "zstd" else cd.zstd_decompress_batch_multi
+            return fn(*self.args(), ws.data_ptr(), ws.numel(), s)
         return cd.BATCH_ENTRIES[fmt](*self.args(), s)
 
     def run_mixed(self, plan, formats, stream=None, tune=False):

@@ -58,6 +58,7 @@ def oracle_lib():
         "oracle_snappy_decode": (ctypes.c_int, _DEC),
         "oracle_lz4f_decode": (ctypes.c_int, _DEC),
         "oracle_zstd_decode": (ctypes.c_int, _DEC),
+        "oracle_zstd_decode_multi": (ctypes.c_int, _DEC),
         "oracle_xxh64": (ctypes.c_uint64, [_U8P, _U64, _U64]),
         "oracle_xxh32": (ctypes.c_uint32, [_U8P, _U64, ctypes.c_uint32]),
         "oracle_lz4_decode_batch": (ctypes.c_int, _BATCH),
@@ -150,6 +151,12 @@ def ref_lz4f_decode(frame, cap):
 def zstd_decode(frame, cap):
     """(status, bytes) from the C restatement of the Zstd frame decode."""
     return _decode_one(oracle_lib().oracle_zstd_decode, frame, cap)
+
+
+def zstd_decode_multi(frames, cap):
+    """(status, bytes) for a buffer of concatenated Zstd and skippable frames,
+    from the C restatement."""
+    return _decode_one(oracle_lib().oracle_zstd_decode_multi, frames, cap)
 
 
 def ref_zstd_decode(frame, cap):

@@ -611,9 +611,12 @@ static int z_repcode(uint64_t* rep, uint64_t ov, uint32_t ll, uint64_t* out) {
     return Z_OK;
 }
 
-int oracle_zstd_decode(const uint8_t* f, uint64_t n, uint8_t* dst, uint64_t cap,
-                       uint64_t* written) {
+/* One frame at the start of f[0, n); *consumed is its length in bytes and
+ * bytes after it are not looked at. */
+static int z_frame(const uint8_t* f, uint64_t n, uint8_t* dst, uint64_t cap,
+                   uint64_t* written, uint64_t* consumed) {
     *written = 0;
+    *consumed = 0;
     if (n < 4) return Z_CORRUPT;
     const uint32_t magic = (uint32_t)z_le(f, 4);
     if (magic != 0xFD2FB528u) {
@@ -782,11 +785,53 @@ int oracle_zstd_decode(const uint8_t* f, uint64_t n, uint8_t* dst, uint64_t cap,
         }
         pos += 4;
     }
-    if (pos != n) { st = Z_CORRUPT; goto done; }
     *written = out;
+    *consumed = pos;
 done:
     free(z);
     free(lit);
     free(seqs);
     return st;
+}
+
+/* One frame per input, the reference's rule (src/zstd_frame.h:196-409):
+ * trailing bytes are CORRUPT, a skippable frame UNSUPPORTED. */
+int oracle_zstd_decode(const uint8_t* f, uint64_t n, uint8_t* dst, uint64_t cap,
+                       uint64_t* written) {
+    uint64_t out = 0, used = 0;
+    *written = 0;
+    const int st = z_frame(f, n, dst, cap, &out, &used);
+    if (st != Z_OK) return st;
+    if (used != n) return Z_CORRUPT;
+    *written = out;
+    return Z_OK;
+}
+
+/* Concatenated frames as libzstd's ZSTD_decompress reads them (the first
+ * rung of the reference's subset ladder, docs/MASTERPLAN.md:1286-1289):
+ * skippable frames (magic 0x184D2A50-5F, 4-byte little-endian size) are
+ * skipped, each Zstd frame decodes after the previous one's output; fewer
+ * than 4 bytes left, or a skippable frame past the end, is CORRUPT. */
+int oracle_zstd_decode_multi(const uint8_t* f, uint64_t n, uint8_t* dst, uint64_t cap,
+                             uint64_t* written) {
+    uint64_t pos = 0, out = 0;
+    *written = 0;
+    while (pos < n) {
+        if (n - pos < 4) return Z_CORRUPT;
+        const uint32_t magic = (uint32_t)z_le(f + pos, 4);
+        if (magic >= 0x184D2A50u && magic <= 0x184D2A5Fu) {
+            if (n - pos < 8) return Z_CORRUPT;
+            const uint64_t sz = z_le(f + pos + 4, 4);
+            if (sz > n - pos - 8) return Z_CORRUPT;
+            pos += 8 + sz;
+            continue;
+        }
+        uint64_t fo = 0, used = 0;
+        const int st = z_frame(f + pos, n - pos, dst + out, cap - out, &fo, &used);
+        if (st != Z_OK) return st;
+        out += fo;
+        pos += used;
+    }
+    *written = out;
+    return Z_OK;
 }

@@ -101,6 +101,16 @@ int main(void) {
         CHECK(cudec_zstd_decompress_batch_noalloc(srcs, sizes, dsts, caps,
                                                   CUDEC_ZSTD_NOALLOC_MAX_CHUNKS + 1, aligned,
                                                   0) == CUDEC_ERR_INVALID_ARGUMENT);
+        /* the multi-frame entry keeps every argument rule */
+        CHECK(cudec_zstd_decompress_batch_multi(srcs, sizes, dsts, caps, 4, aligned, 0, ws, 0) ==
+              CUDEC_ERR_INVALID_ARGUMENT);
+        CHECK(cudec_zstd_decompress_batch_multi(srcs, sizes, dsts, caps, 4, aligned, storage,
+                                                ws - 1, 0) == CUDEC_ERR_INVALID_ARGUMENT);
+        CHECK(cudec_zstd_decompress_batch_multi(
+                  srcs, sizes, dsts, caps, 4, (cudec_chunk_result*)((unsigned char*)aligned + 8),
+                  storage, ws, 0) == CUDEC_ERR_INVALID_ARGUMENT); /* misaligned records */
+        CHECK(cudec_zstd_decompress_batch_multi(srcs, sizes, dsts, caps, 0, aligned, storage, ws,
+                                                0) == CUDEC_ERR_INVALID_ARGUMENT);
     }
 
     /* GDeflate TileStream: the envelope walker is host-only */
