@@ -57,6 +57,7 @@ constexpr int kBuckets = CUDEC_MIXED_BUCKETS;
 constexpr int kSizeClasses = 64;  // floor(log2(capacity)) classes for the order
 constexpr int kClasses = 2 * kSizeClasses;  // CTA-decoded chunks: the upper half
 constexpr uint32_t kCtaWarps = lzc::kWarps;  // warps per chunk of the CTA decoder
+static_assert(kCtaWarps == CUDEC_MIXED_CTA_WARPS, "the ABI's whole-CTA warps value");
 constexpr uint32_t kCtaSmem = kMaxOf(static_cast<uint32_t>(sizeof(lzc::Shm<lzc::Lz4F>)),
                                      static_cast<uint32_t>(sizeof(lzc::Shm<lzc::SnappyF>)));
 static_assert(kWarpSmem % 16 == 0, "per-warp regions stay 16-byte aligned");

@@ -237,6 +237,10 @@ typedef enum cudec_format {
  * < 16 KiB, < 64 KiB, < 256 KiB, < 1 MiB, larger. */
 #define CUDEC_MIXED_BUCKETS 6
 
+/* Warps of the CTA-per-chunk LZ4 / Snappy decoder (the whole-CTA value of a
+ * decode shape's warps per chunk). */
+#define CUDEC_MIXED_CTA_WARPS 4
+
 typedef struct cudec_mixed_plan cudec_mixed_plan;
 
 cudec_status cudec_mixed_plan_create(cudec_mixed_plan** out_plan);
@@ -273,14 +277,15 @@ cudec_status cudec_mixed_plan_get_tuning(const cudec_mixed_plan* plan,
                                          uint32_t* out_params);
 
 /* The whole decode shape, 4 values per bucket b: out_shape[4*b] = warps per
- * LZ4 / Snappy chunk (1: one warp; 8: a whole CTA runs the CTA-per-chunk
- * decoder), then parse reach, lookahead and ring batch of the one-warp
- * decoder. A plan starts from a compiled-in table (a CTA per LZ4 / Snappy
- * chunk in every bucket); cudec_mixed_plan_tune measures one on the caller's
- * chunks. A caller can save the shape and set it on later plans, so the
- * decode shape is fixed across runs; set_shape refuses (INVALID_ARGUMENT,
- * nothing changed) a warps value other than 1 or 8 or an out-of-range
- * one-warp shape. Any shape decodes identically; it only moves time. */
+ * LZ4 / Snappy chunk (1: one warp; CUDEC_MIXED_CTA_WARPS: a whole CTA runs
+ * the CTA-per-chunk decoder), then parse reach, lookahead and ring batch of
+ * the one-warp decoder. A plan starts from a compiled-in table (a CTA per
+ * LZ4 / Snappy chunk in every bucket); cudec_mixed_plan_tune measures one on
+ * the caller's chunks. A caller can save the shape and set it on later
+ * plans, so the decode shape is fixed across runs; set_shape refuses
+ * (INVALID_ARGUMENT, nothing changed) a warps value other than 1 or
+ * CUDEC_MIXED_CTA_WARPS, or an out-of-range one-warp shape. Any shape
+ * decodes identically; it only moves time. */
 cudec_status cudec_mixed_plan_get_shape(const cudec_mixed_plan* plan, uint32_t* out_shape);
 cudec_status cudec_mixed_plan_set_shape(cudec_mixed_plan* plan, const uint32_t* shape);
 

@@ -127,9 +127,9 @@ def test_warps_per_chunk_shapes_agree(cuda):
     recs, outs = per_format(cuda, comps, caps, fmts)
     plan = cd.MixedPlan()
     default = plan.shape()
-    assert [s[0] for s in default] == [8, 8, 8, 8, 8, 8]
+    assert [s[0] for s in default] == [cd.MIXED_CTA_WARPS] * 6
     b = DeviceBatch(comps, caps, device=cuda)
-    for wpc in (1, 8, None):
+    for wpc in (1, cd.MIXED_CTA_WARPS, None):
         shape = default if wpc is None else [(wpc,) + tuple(s[1:]) for s in default]
         assert plan.set_shape(shape) == 0
         assert plan.shape() == [tuple(s) for s in shape]
@@ -138,7 +138,7 @@ def test_warps_per_chunk_shapes_agree(cuda):
         torch.cuda.synchronize()
         check(b, recs, outs, "warps per chunk %s" % wpc)
     bad = [list(s) for s in default]
-    bad[2][0] = 4
+    bad[2][0] = 2
     assert plan.set_shape(bad) == cd.ERR_INVALID_ARGUMENT
     bad = [list(s) for s in default]
     bad[0][1] = 7
@@ -158,7 +158,7 @@ def test_tuner_keeps_results_and_reports_valid_shapes(cuda):
     check(b, recs, outs, "tuning run")
     for pw, ahead, batch in plan.tuning():
         assert pw in (256, 512, 1024) and pw + 64 <= ahead <= 4032 and batch in (2048, 4096)
-    assert all(s[0] in (1, 8) for s in plan.shape())
+    assert all(s[0] in (1, cd.MIXED_CTA_WARPS) for s in plan.shape())
     b.reset()
     assert b.run_mixed(plan, fmts) == 0
     torch.cuda.synchronize()
