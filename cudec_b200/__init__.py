@@ -234,7 +234,7 @@ FORMAT_LZ4, FORMAT_SNAPPY, FORMAT_ZSTD, FORMAT_GDEFLATE = 0, 1, 2, 3
 FORMAT_CODES = {"lz4": FORMAT_LZ4, "snappy": FORMAT_SNAPPY, "zstd": FORMAT_ZSTD,
                 "gdeflate": FORMAT_GDEFLATE}
 MIXED_BUCKETS = 6
-MIXED_CTA_WARPS = 4  # CUDEC_MIXED_CTA_WARPS: warps of the CTA-per-chunk decoder
+MIXED_CTA_WARPS = 8  # CUDEC_MIXED_CTA_WARPS: warps of the CTA-per-chunk decoder
 
 
 class MixedPlan:

@@ -30,29 +30,26 @@
 //      first failing or terminal token (a block-wide minimum) decides the
 //      chunk exactly as the serial parser would, since the steps equal the
 //      ladder's next position for every token the ladder accepts;
-//   7. execute, in groups of consecutive tokens whose output fits kGroupOut
-//      counted from the destination block holding the group's first byte:
-//      thread t assembles the group's t-th 16-byte destination block in an
-//      output ring in shared memory (indexed by destination address mod
-//      kRing, so ring blocks and destination blocks share alignment). Each
-//      byte gets its value (a literal, or a match byte whose source precedes
-//      the group) or a pointer to the group byte it copies (the period of a
-//      match maps every match byte before the match); pointer jumping then
-//      shortens every chain to one hop in a few barrier rounds, and each
-//      pointed byte copies its source. Completed aligned 16-byte blocks
-//      leave the ring as coalesced stores. A token longer than kBig is
-//      copied by the whole CTA straight to the destination. Sources older
-//      than the ring are read back from the destination.
+//   7. execute, in groups of consecutive tokens whose output fits kGroupOut:
+//      the group's literal runs are copied into an output ring in shared
+//      memory (indexed by destination address mod kRing, so ring blocks and
+//      destination blocks share alignment), then its matches as data flow:
+//      each thread copies each of its matches once none of the bytes its
+//      source reads is the output of a match still pending in the group (a
+//      bit per output byte), and clears the match's own bits after its bytes
+//      land; the lowest pending match is always ready, so the group always
+//      makes progress.
+//      Completed aligned 16-byte blocks leave the ring as coalesced stores.
+//      A token longer than kBig is copied by the whole CTA straight to the
+//      destination. Sources older than the ring are read back from the
+//      destination.
 //
 // Every phase is per-thread code between CTA barriers, driven through an
 // executor: on the device each phase runs once per thread followed by
 // __syncthreads(); the host executor runs the phases for every thread in
-// turn, which emulates one interleaving of the CTA: a phase reads what
-// another thread writes in the same phase only where every interleaving
-// gives the same result (atomics whose order does not matter; a pointer
-// jumping round, which reads a pointer or a later one on the same chain;
-// bytes rewritten with the value they hold). The host emulation is what the
-// CPU tests run.
+// turn, which emulates the CTA exactly (no phase reads what another thread
+// writes in the same phase, except through atomics whose order does not
+// change the result). The host emulation is what the CPU tests run.
 //
 // Statuses follow the reference ladders exactly: LZ4 iderex/cudec
 // src/lz4_block.h:95-258, Snappy src/snappy_block.h:172-435.
@@ -67,8 +64,8 @@
 namespace cdb {
 namespace lzc {
 
-constexpr uint32_t kThreads = 128;                 // threads per CTA
-constexpr uint32_t kCtasPerSm = 8;                 // resident CTAs per SM the registers allow
+constexpr uint32_t kThreads = 256;                 // threads per CTA
+constexpr uint32_t kCtasPerSm = 4;                 // resident CTAs per SM the registers allow
 constexpr uint32_t kWarps = kThreads / 32;
 constexpr uint32_t kSeg = 16;                      // positions per segment (one per thread)
 constexpr uint32_t kTile = kThreads * kSeg;        // positions per tile
@@ -79,12 +76,16 @@ constexpr uint32_t kCand = 32;                     // candidate entries per supe
 constexpr uint32_t kLook = 512;                    // staged bytes past the tile
 constexpr uint32_t kInBytes = kTile + kLook + 32;  // staged input (aligned blocks)
 constexpr uint32_t kExIdx = kTile + kTile / 16;    // exits, one pad word per 16
-constexpr uint32_t kRing = 8192;                   // output ring (bytes)
-constexpr uint32_t kSpinCap = 1u << 22;            // data-flow passes a thread makes over its matches
+constexpr uint32_t kRing = 16384;                  // output ring (bytes)
+constexpr uint32_t kGroupOut = 4096;               // output bytes per execution group
+constexpr uint32_t kPerThread = 2;                 // tokens per thread per group
+constexpr uint32_t kGroupTok = kThreads * kPerThread;
 constexpr uint32_t kBig = 256;                     // longer tokens: whole-CTA copies
 constexpr uint32_t kExtCap = 16;                   // extension bytes a segment step reads
+constexpr uint32_t kSpinCap = 1u << 22;            // passes a thread makes over its matches
 
 static_assert(kSupers == kWarps, "one super-segment per warp");
+static_assert(kGroupOut + 32 <= kRing, "a group and its clear margin fit the ring");
 static_assert(kInBytes % 16 == 0, "staging in 16-byte blocks");
 
 // Exit codes of the segment walk (relative positions otherwise).
@@ -231,26 +232,6 @@ CDB_HD void zero16(uint8_t* p) {  // 16-byte aligned
 #endif
 }
 
-// Four words from / to 16-byte aligned shared memory.
-CDB_HD void ld_words(const uint8_t* p, uint32_t* w) {
-#if defined(__CUDA_ARCH__)
-    const uint4 v = *reinterpret_cast<const uint4*>(p);
-    w[0] = v.x;
-    w[1] = v.y;
-    w[2] = v.z;
-    w[3] = v.w;
-#else
-    std::memcpy(w, p, 16);
-#endif
-}
-CDB_HD void st_words(uint8_t* p, const uint32_t* w) {
-#if defined(__CUDA_ARCH__)
-    *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
-#else
-    std::memcpy(p, w, 16);
-#endif
-}
-
 // The first m (1..16) bytes of v at global address p.
 CDB_HD void put_global(uint8_t* p, const V16& v, uint32_t m) {
 #if defined(__CUDA_ARCH__)
@@ -274,10 +255,6 @@ CDB_HD void put_global(uint8_t* p, const V16& v, uint32_t m) {
 struct Lz4F : lzl::Lz4Ladder {
     static constexpr uint32_t kMaxTok = kTile / 3 + 3;  // tokens with a successor span >= 3 bytes
     static constexpr bool kSnappy = false;
-    // execution: matches as data flow, 3 tokens per thread, 4 KiB groups
-    static constexpr bool kFlow = true;
-    static constexpr uint32_t kPerThread = 3;
-    static constexpr uint32_t kGroupOut = 4096;
 
     template <class R>
     CDB_HD static uint64_t step(const R& in, uint64_t S, uint64_t P, uint32_t cap,
@@ -381,11 +358,6 @@ struct Lz4F : lzl::Lz4Ladder {
 struct SnappyF : lzl::SnappyLadder {
     static constexpr uint32_t kMaxTok = kTile / 2 + 3;  // elements span >= 2 bytes
     static constexpr bool kSnappy = true;
-    // execution: pointer jumping, 4 tokens per thread, a 16-byte
-    // destination block per thread
-    static constexpr bool kFlow = false;
-    static constexpr uint32_t kPerThread = 4;
-    static constexpr uint32_t kGroupOut = kThreads * 16;
 
     template <class R>
     CDB_HD static uint64_t step(const R& in, uint64_t S, uint64_t P, uint32_t,
@@ -480,45 +452,10 @@ struct SnappyF : lzl::SnappyLadder {
 };
 
 // ---------------------------------------------------------------------------
-// The tile's token records and the execution state of a group, per
-// execution scheme. Data flow: 32-bit records, a token's position field
-// reused for the in-group part of its match source, a pending bit per group
-// byte. Pointer jumping: 16-bit positions and lengths (lengths saturate;
-// longer tokens are re-read by the ladder) and a pointer per group byte.
-template <class F, bool Flow = F::kFlow>
-struct TokRecs;
-template <class F>
-struct TokRecs<F, true> {
-    static constexpr uint32_t kMaxTok = F::kMaxTok;
-    static constexpr uint64_t kSat = 0xFFFFFFFFull;
-    uint32_t pos[kMaxTok];  // token position - e; during execution, the match's in-group source
-    uint32_t lit[kMaxTok];  // saturated at kSat
-    uint32_t ml[kMaxTok];
-    uint32_t off[kMaxTok];
-    uint32_t out[kMaxTok];  // output offset - d0
-    uint32_t pend_bits[F::kGroupOut / 32 + 8];  // per group byte: pending
-    uint8_t pend[kThreads];                     // per thread: its pending matches
-};
-template <class F>
-struct TokRecs<F, false> {
-    static constexpr uint32_t kMaxTok = F::kMaxTok;
-    static constexpr uint64_t kSat = 0xFFFFull;
-    uint32_t off[kMaxTok];
-    uint32_t out[kMaxTok];  // output offset - d0
-    uint16_t pos[kMaxTok];  // token position - e (< kTile)
-    uint16_t lit[kMaxTok];  // saturated at kSat
-    uint16_t ml[kMaxTok];
-    alignas(16) uint16_t ptr[F::kGroupOut];  // per group byte: the byte it copies
-};
-
-// ---------------------------------------------------------------------------
 // Shared memory of one CTA.
 template <class F>
 struct Shm {
     static constexpr uint32_t kMaxTok = F::kMaxTok;
-    static constexpr uint32_t kGroupTok = kThreads * F::kPerThread;
-    static_assert(F::kGroupOut + 32 <= kRing, "a group and its clear margin fit the ring");
-    static_assert(F::kFlow || F::kGroupOut == kThreads * 16, "pointer jumping: a block per thread");
     alignas(16) uint8_t in[kInBytes];  // staged input: positions [ibase, ibase + kInBytes)
     union {
         struct {
@@ -527,12 +464,20 @@ struct Shm {
             uint32_t cand_exit[kSupers][kCand];
             uint8_t ovr[kSupers][kSupSegs];       // exact-walk entries
         } p;
-        TokRecs<F> t;
+        struct {
+            uint32_t pos[kMaxTok];  // token position - e
+            uint32_t lit[kMaxTok];  // saturated at 2^32 - 1
+            uint32_t ml[kMaxTok];
+            uint32_t off[kMaxTok];
+            uint32_t out[kMaxTok];  // output offset - d0
+        } t;
     } u;
     alignas(16) uint8_t ring[kRing];
+    uint32_t pend_bits[kGroupOut / 32 + 8];
     uint32_t seg_entry[kThreads];  // relative entry, or kUnknown for none
     uint32_t seg_cnt[kThreads];    // tokens; after the scan, the first token's index
     uint64_t seg_olen[kThreads];   // output bytes; after the scan, the first token's offset
+    uint8_t pend[kThreads];        // per-thread pending match masks
     uint8_t chosen[kSupers];
     uint32_t wsum_c[kWarps];  // block scan: per-warp totals
     uint64_t wsum_o[kWarps];
@@ -975,10 +920,9 @@ struct Chunk {
                     ol = 0;
                     nx = next_of(in, b, lim, P, &ol);
                 }
-                constexpr uint64_t kSat = TokRecs<F>::kSat;
                 s.u.t.pos[i] = static_cast<uint32_t>(P - e);
-                s.u.t.lit[i] = static_cast<uint32_t>(sq.lit > kSat ? kSat : sq.lit);
-                s.u.t.ml[i] = static_cast<uint32_t>(sq.ml > kSat ? kSat : sq.ml);
+                s.u.t.lit[i] = sq.lit > 0xFFFFFFFFull ? 0xFFFFFFFFu : static_cast<uint32_t>(sq.lit);
+                s.u.t.ml[i] = sq.ml > 0xFFFFFFFFull ? 0xFFFFFFFFu : static_cast<uint32_t>(sq.ml);
                 s.u.t.off[i] = sq.off;
                 s.u.t.out[i] = static_cast<uint32_t>(o);
                 // the first failing or terminal token ends the chunk; a step
@@ -1083,7 +1027,7 @@ struct Chunk {
             uint32_t m = ~0u;
             if (w == a >> 5) m &= ~0u << (a & 31);
             if (w == (b - 1) >> 5) m &= ~0u >> (31 - ((b - 1) & 31));
-            if (*static_cast<volatile uint32_t*>(&s.u.t.pend_bits[w]) & m) return false;
+            if (*static_cast<volatile uint32_t*>(&s.pend_bits[w]) & m) return false;
         }
         return true;
     }
@@ -1092,8 +1036,8 @@ struct Chunk {
             uint32_t m = ~0u;
             if (w == a >> 5) m &= ~0u << (a & 31);
             if (w == (b - 1) >> 5) m &= ~0u >> (31 - ((b - 1) & 31));
-            if (set) at_or(&s.u.t.pend_bits[w], m);
-            else at_and(&s.u.t.pend_bits[w], ~m);
+            if (set) at_or(&s.pend_bits[w], m);
+            else at_and(&s.pend_bits[w], ~m);
         }
     }
 
@@ -1118,8 +1062,8 @@ struct Chunk {
     }
 
     // Tokens [g0, g1), all of at most kBig bytes, output [G0, G1) within
-    // F::kGroupOut: literals, then matches as data flow, through the ring.
-    CDB_HD void exec_group_flow(uint32_t g0, uint32_t g1) {
+    // kGroupOut: literals, then matches in rounds, through the ring.
+    CDB_HD void exec_group(uint32_t g0, uint32_t g1) {
         const Reader in = reader();
         const Ring rg = ring();
         const uint64_t d0 = s.d0, e = s.e;
@@ -1141,12 +1085,12 @@ struct Chunk {
             const uint32_t end = ib + span;
             for (uint32_t q = (ib & ~15u) + 16 + 16 * t; q < end; q += 16 * kThreads)
                 zero16(s.ring + (q & (kRing - 1)));
-            for (uint32_t w = t; w < F::kGroupOut / 32 + 8; w += kThreads) s.u.t.pend_bits[w] = 0;
+            for (uint32_t w = t; w < kGroupOut / 32 + 8; w += kThreads) s.pend_bits[w] = 0;
         });
         // literals; pending bits of the matches
         each([&](uint32_t t) {
             uint8_t pm = 0;
-            for (uint32_t k = 0; k < F::kPerThread; ++k) {
+            for (uint32_t k = 0; k < kPerThread; ++k) {
                 const uint32_t i = g0 + t + k * kThreads;
                 if (i >= g1) break;
                 const uint32_t lit = s.u.t.lit[i], ml = s.u.t.ml[i];
@@ -1173,7 +1117,7 @@ struct Chunk {
                                            : 0u;
                 }
             }
-            s.u.t.pend[t] = pm;
+            s.pend[t] = pm;
         });
         LZC_PHASE(6);
         LZC_EVENT(3, 1);
@@ -1184,12 +1128,12 @@ struct Chunk {
         // over the CTA makes progress; passes per thread are bounded.
 #if defined(__CUDA_ARCH__)
         each([&](uint32_t t) {
-            uint8_t pm = s.u.t.pend[t];
+            uint8_t pm = s.pend[t];
             uint32_t spin = 0;
             for (; pm; ++spin) {
                 // a thread's matches in order (its lowest pending first): a
                 // warp's lanes then hold consecutive tokens and copy together
-                for (uint32_t k = 0; k < F::kPerThread; ++k)
+                for (uint32_t k = 0; k < kPerThread; ++k)
                     if (pm & (1u << k)) {
                         if (try_match(rg, g0 + t + k * kThreads, G0))
                             pm = static_cast<uint8_t>(pm & ~(1u << k));
@@ -1208,11 +1152,11 @@ struct Chunk {
         for (uint32_t pass = 0;; ++pass) {
             bool any = false;
             for (uint32_t t = 0; t < kThreads; ++t) {
-                uint8_t pm = s.u.t.pend[t];
-                for (uint32_t k = 0; k < F::kPerThread; ++k)
+                uint8_t pm = s.pend[t];
+                for (uint32_t k = 0; k < kPerThread; ++k)
                     if ((pm & (1u << k)) && try_match(rg, g0 + t + k * kThreads, G0))
                         pm = static_cast<uint8_t>(pm & ~(1u << k));
-                s.u.t.pend[t] = pm;
+                s.pend[t] = pm;
                 any = any || pm != 0;
             }
             if (!any) break;
@@ -1223,155 +1167,6 @@ struct Chunk {
         }
 #endif
         LZC_EVENT(2, 1);
-        LZC_PHASE(7);
-        flush(G1, false);
-        each([&](uint32_t t) {
-            if (t == 0) s.dend = G1;
-        });
-        LZC_PHASE(8);
-    }
-
-    // Tokens [g0, g1), all of at most kBig bytes, output [G0, G1); A0 is G0
-    // rounded down to a destination block and G1 - A0 <= F::kGroupOut:
-    //   1. two tokens per thread: literal runs, and matches whose source
-    //      precedes the group, are copied into the ring 16 bytes at a time;
-    //      a match reading the group gives each byte whose source is in the
-    //      group a pointer to that byte (byte x of a match reads
-    //      period[(x - ms) mod off], so the pointer lies before the match)
-    //      and copies the others;
-    //   2. pointer jumping, thread t over the 16 pointers of destination
-    //      block t: each pointer takes its target's pointer until the target
-    //      is a byte with a value (chains halve per round);
-    //   3. each pointed byte copies its target; the block is rewritten whole.
-    CDB_HD void exec_group_jump(uint32_t g0, uint32_t g1) {
-        constexpr uint16_t kDone = 0xFFFF;
-        const Reader in = reader();
-        const Ring rg = ring();
-        const uint64_t d0 = s.d0, e = s.e;
-        const uint64_t G0 = d0 + s.u.t.out[g0];
-        const uint64_t G1 = d0 + s.u.t.out[g1 - 1] + s.u.t.lit[g1 - 1] + s.u.t.ml[g1 - 1];
-        const uint32_t mis = static_cast<uint32_t>((rg.dbase + G0) & 15);
-        const uint64_t A0 = G0 - mis;
-        const uint32_t span = static_cast<uint32_t>(G1 - A0);
-        uint16_t* const ptr = s.u.t.ptr;
-        // the clear below may zero up to 15 bytes past G1, whose slots held
-        // positions up to G1 + 15 - kRing: those are read back from dst
-        each([&](uint32_t t) {
-            if (t == 0 && G1 + 16 > s.vlo + kRing) s.vlo = G1 + 16 - kRing;
-        });
-        // clear the group's ring bytes (keeping the first block's bytes
-        // before G0) and its pointers
-        const uint32_t ib = rg.idx(G0);
-        each([&](uint32_t t) {
-            uint32_t* r32 = reinterpret_cast<uint32_t*>(s.ring);
-            const uint32_t w0 = ib >> 2;
-            if (t == 0) at_and(r32 + w0, (1u << (8 * (ib & 3))) - 1);
-            if (t >= 1 && t < 4 - (w0 & 3)) r32[w0 + t] = 0;
-            const uint32_t end = ib + (span - mis);
-            for (uint32_t q = (ib & ~15u) + 16 + 16 * t; q < end; q += 16 * kThreads)
-                zero16(s.ring + (q & (kRing - 1)));
-            const uint32_t dn[4] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu};
-            st_words(reinterpret_cast<uint8_t*>(ptr + 16 * t), dn);
-            st_words(reinterpret_cast<uint8_t*>(ptr + 16 * t + 8), dn);
-        });
-        const uint64_t vlo = s.vlo;
-        bool pending = each_or([&](uint32_t t) -> bool {
-            bool any = false;
-            for (uint32_t k = 0; k < F::kPerThread; ++k) {
-                const uint32_t i = g0 + t + k * kThreads;
-                if (i >= g1) break;
-                const uint32_t lit = s.u.t.lit[i], ml = s.u.t.ml[i];
-                const uint64_t o = d0 + s.u.t.out[i];
-                if (lit) {
-                    const uint64_t ls = F::lit_src(in, e + s.u.t.pos[i], lit);
-                    for (uint32_t q = 0; q < lit; q += 16) {
-                        const uint32_t m = lit - q < 16 ? lit - q : 16u;
-                        rg.put16(o + q, in16(in, ls + q, m), m);
-                    }
-                }
-                if (!ml) continue;
-                const uint32_t off = s.u.t.off[i];
-                const uint64_t ms = o + lit;
-                if (ms - off + (ml < off ? ml : off) <= G0) {  // the source precedes the group
-                    copy_match_ring(rg, ms, ml, off);
-                    continue;
-                }
-                uint32_t ph = 0;
-                for (uint32_t q = 0; q < ml; ++q) {
-                    const uint64_t src = ms - off + ph;
-                    ph = ph + 1 == off ? 0 : ph + 1;
-                    const uint64_t x = ms + q;
-                    if (src >= G0) {
-                        ptr[x - A0] = static_cast<uint16_t>(src - A0);
-                        any = true;
-                    } else {
-                        const uint32_t v = src >= vlo ? rg.ring[rg.idx(src)] : dst[src];
-                        const uint32_t ix = rg.idx(x);
-                        at_or(reinterpret_cast<uint32_t*>(s.ring) + (ix >> 2), v << (8 * (ix & 3)));
-                    }
-                }
-            }
-            return any;
-        });
-        LZC_PHASE(6);
-        LZC_EVENT(3, 1);
-        // a synchronous round at least halves every chain, and in-place
-        // updates only shorten them: at most 13 rounds for 4096 bytes
-        for (uint32_t round = 0; pending; ++round) {
-            if (round > 16) {  // unreachable: see above
-                each([&](uint32_t t) {
-                    if (t == 0) s.status = CUDEC_ERR_CUDA;
-                });
-                return;
-            }
-            LZC_EVENT(2, 1);
-            pending = each_or([&](uint32_t t) -> bool {
-                const uint32_t r0 = 16 * t;
-                if (r0 >= span) return false;
-                uint32_t pw[8];
-                ld_words(reinterpret_cast<const uint8_t*>(ptr + r0), pw);
-                ld_words(reinterpret_cast<const uint8_t*>(ptr + r0 + 8), pw + 4);
-                bool changed = false, open = false;
-#pragma unroll
-                for (uint32_t j = 0; j < 16; ++j) {
-                    const uint32_t p = (pw[j >> 1] >> (16 * (j & 1))) & 0xFFFFu;
-                    if (p == kDone) continue;
-                    // a pointer never becomes kDone: once read as kDone,
-                    // the source's value is final
-                    const uint32_t q = ptr[p];
-                    if (q == kDone) continue;
-                    pw[j >> 1] = (pw[j >> 1] & ~(0xFFFFu << (16 * (j & 1)))) | (q << (16 * (j & 1)));
-                    changed = true;
-                    open = open || ptr[q] != kDone;
-                }
-                if (changed) {
-                    st_words(reinterpret_cast<uint8_t*>(ptr + r0), pw);
-                    st_words(reinterpret_cast<uint8_t*>(ptr + r0 + 8), pw + 4);
-                }
-                return open;
-            });
-        }
-        each([&](uint32_t t) {
-            const uint32_t r0 = 16 * t;
-            if (r0 >= span) return;
-            uint32_t pw[8];
-            ld_words(reinterpret_cast<const uint8_t*>(ptr + r0), pw);
-            ld_words(reinterpret_cast<const uint8_t*>(ptr + r0 + 8), pw + 4);
-            bool any = false;
-            for (uint32_t j = 0; j < 8; ++j) any = any || pw[j] != 0xFFFFFFFFu;
-            if (!any) return;
-            uint8_t* const blk = s.ring + rg.idx(A0 + r0);
-            uint32_t w[4];
-            ld_words(blk, w);
-#pragma unroll
-            for (uint32_t j = 0; j < 16; ++j) {
-                const uint32_t p = (pw[j >> 1] >> (16 * (j & 1))) & 0xFFFFu;
-                if (p == kDone) continue;
-                const uint32_t v = rg.ring[rg.idx(A0 + p)];
-                w[j >> 2] = (w[j >> 2] & ~(0xFFu << (8 * (j & 3)))) | (v << (8 * (j & 3)));
-            }
-            st_words(blk, w);
-        });
         LZC_PHASE(7);
         flush(G1, false);
         each([&](uint32_t t) {
@@ -1449,21 +1244,17 @@ struct Chunk {
         uint32_t g0 = 0;
         while (g0 < ne && s.status == CUDEC_OK) {
             // the group: up to kGroupTok tokens, cut at a big token or where
-            // the output passes the format's group size (pointer jumping:
-            // counted from the destination block holding its first byte)
-            constexpr uint32_t kGroupTok = Shm<F>::kGroupTok;
+            // the output passes kGroupOut
             const uint32_t lim = ne - g0 < kGroupTok ? ne : g0 + kGroupTok;
             const uint32_t o0 = s.u.t.out[g0];
-            const uint32_t mis = F::kFlow ? 0u : static_cast<uint32_t>(
-                (reinterpret_cast<uintptr_t>(dst) + s.d0 + o0) & 15);
             each([&](uint32_t t) {
                 if (t == 0) s.cut = lim;
             });
             each([&](uint32_t t) {
                 for (uint32_t i = g0 + t; i < lim; i += kThreads) {
-                    const uint64_t end = static_cast<uint64_t>(s.u.t.out[i]) - o0 + mis +
+                    const uint64_t end = static_cast<uint64_t>(s.u.t.out[i]) - o0 +
                                          s.u.t.lit[i] + s.u.t.ml[i];
-                    if (is_big(i) || end > F::kGroupOut) {
+                    if (is_big(i) || end > kGroupOut) {
                         at_min(&s.cut, i);
                         break;
                     }
@@ -1475,8 +1266,7 @@ struct Chunk {
                 exec_big(g0);
                 g0 += 1;
             } else {
-                if constexpr (F::kFlow) exec_group_flow(g0, c);
-                else exec_group_jump(g0, c);
+                exec_group(g0, c);
                 g0 = c;
             }
         }

@@ -239,7 +239,7 @@ typedef enum cudec_format {
 
 /* Warps of the CTA-per-chunk LZ4 / Snappy decoder (the whole-CTA value of a
  * decode shape's warps per chunk). */
-#define CUDEC_MIXED_CTA_WARPS 4
+#define CUDEC_MIXED_CTA_WARPS 8
 
 typedef struct cudec_mixed_plan cudec_mixed_plan;
 
