@@ -16,10 +16,14 @@ namespace zstd {
 
 constexpr uint32_t kMaxSlots = 4096;  // frames decoded concurrently (workspace slots)
 
+// Multi: a chunk is a sequence of frames (decode_frames) rather than one
+// frame (decode_frame); a template parameter, so the one-frame kernel is
+// compiled alone.
+template <bool Multi>
 __global__ void __launch_bounds__(kCtaThreads)
     zstd_decode_kernel(const void* const* src_ptrs, const size_t* src_sizes,
                        void* const* dst_ptrs, const size_t* dst_caps, size_t n,
-                       cudec_chunk_result* results, uint8_t* workspace, bool multi = false) {
+                       cudec_chunk_result* results, uint8_t* workspace) {
     __shared__ WarpSmem wsm[kWarpsPerCta];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const size_t gw = static_cast<size_t>(blockIdx.x) * kWarpsPerCta + warp;
@@ -29,10 +33,13 @@ __global__ void __launch_bounds__(kCtaThreads)
         uint64_t written = 0;
         const uint8_t* src = static_cast<const uint8_t*>(src_ptrs[c]);
         uint8_t* dst = static_cast<uint8_t*>(dst_ptrs[c]);
-        const int st = multi ? decode_frames(src, src_sizes[c], dst, dst_caps[c], wsm[warp],
-                                             litbuf, lane, &written)
-                             : decode_frame(src, src_sizes[c], dst, dst_caps[c], wsm[warp],
-                                            litbuf, lane, &written);
+        int st;
+        if constexpr (Multi)
+            st = decode_frames(src, src_sizes[c], dst, dst_caps[c], wsm[warp], litbuf, lane,
+                               &written);
+        else
+            st = decode_frame(src, src_sizes[c], dst, dst_caps[c], wsm[warp], litbuf, lane,
+                              &written);
         __syncwarp();
         if (lane == 0) {
             results[c].status = st;
@@ -70,10 +77,11 @@ cudec_status launch_zstd(const void* const* d_src_ptrs, const size_t* d_src_size
     (void)cudaGetLastError();
     const size_t slots = cudec_zstd_workspace_bytes(chunk_count) / cdb::zstd::kLitSlot;
     const unsigned grid = static_cast<unsigned>(slots / cdb::zstd::kWarpsPerCta);
-    cdb::zstd::zstd_decode_kernel<<<grid, cdb::zstd::kCtaThreads, 0,
-                                    reinterpret_cast<cudaStream_t>(stream)>>>(
+    const auto kernel = multi ? cdb::zstd::zstd_decode_kernel<true>
+                              : cdb::zstd::zstd_decode_kernel<false>;
+    kernel<<<grid, cdb::zstd::kCtaThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_capacities, chunk_count, d_results,
-        static_cast<uint8_t*>(d_workspace), multi);
+        static_cast<uint8_t*>(d_workspace));
     return cudaGetLastError() == cudaSuccess ? CUDEC_OK : CUDEC_ERR_CUDA;
 }
 
@@ -167,8 +175,8 @@ extern "C" cudec_status cudec_zstd_decompress_batch_noalloc(
     }
     const unsigned grid = static_cast<unsigned>(
         (chunk_count + cdb::zstd::kWarpsPerCta - 1) / cdb::zstd::kWarpsPerCta);
-    cdb::zstd::zstd_decode_kernel<<<grid, cdb::zstd::kCtaThreads, 0,
-                                    reinterpret_cast<cudaStream_t>(stream)>>>(
+    cdb::zstd::zstd_decode_kernel<false><<<grid, cdb::zstd::kCtaThreads, 0,
+                                           reinterpret_cast<cudaStream_t>(stream)>>>(
         d_src_ptrs, d_src_sizes, d_dst_ptrs, d_dst_capacities, chunk_count, d_results, slots);
     return cudaGetLastError() == cudaSuccess ? CUDEC_OK : CUDEC_ERR_CUDA;
 }
