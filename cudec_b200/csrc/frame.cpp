@@ -16,8 +16,12 @@
 // mark, optional content checksum), XXH32 with seed 0 throughout.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <atomic>
 #include <cstring>
+#include <functional>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "cudec.h"
@@ -48,6 +52,68 @@ struct Block {
     bool raw;  // stored uncompressed
 };
 
+// Block checksums of a frame, verified on host threads while the device
+// decodes the blocks: every block is independent, and any mismatch is the
+// same CORRUPT_INPUT that the walk would have returned at that block, so the
+// order of the checks does not show. Frames with less than kParallelBytes of
+// blocks are verified by the calling thread.
+class BlockSums {
+  public:
+    static constexpr size_t kParallelBytes = size_t{4} << 20;
+
+    BlockSums(const unsigned char* f, const std::vector<Block>& blocks, bool present)
+        : f_(f), blocks_(blocks) {
+        if (!present || blocks.empty()) return;
+        size_t bytes = 0;
+        for (const Block& b : blocks) bytes += b.len;
+        unsigned hw = std::thread::hardware_concurrency();
+        const size_t nt = std::min<size_t>({hw ? hw : 1u, 16u, blocks.size()});
+        if (bytes < kParallelBytes || nt < 2) {
+            ok_ = check(0, 1);
+            return;
+        }
+        try {
+            for (size_t t = 0; t < nt; ++t)
+                threads_.emplace_back([this, t, nt] {
+                    if (!check(t, nt)) bad_.store(true, std::memory_order_relaxed);
+                });
+        } catch (...) {  // no thread to be had: the rest on this one
+            const size_t started = threads_.size();
+            for (size_t t = started; t < nt; ++t)
+                if (!check(t, nt)) bad_.store(true, std::memory_order_relaxed);
+        }
+    }
+    ~BlockSums() { join(); }
+    BlockSums(const BlockSums&) = delete;
+    BlockSums& operator=(const BlockSums&) = delete;
+
+    // Whether every block checksum matched (waits for the threads).
+    bool ok() {
+        join();
+        return ok_ && !bad_.load(std::memory_order_relaxed);
+    }
+
+  private:
+    // Blocks t, t + nt, ...: the 4-byte checksum follows each block.
+    bool check(size_t t, size_t nt) const {
+        for (size_t i = t; i < blocks_.size(); i += nt) {
+            const Block& b = blocks_[i];
+            if (xxh32(f_ + b.off, b.len) != rd32(f_ + b.off + b.len)) return false;
+        }
+        return true;
+    }
+    void join() {
+        for (std::thread& th : threads_)
+            if (th.joinable()) th.join();
+    }
+
+    const unsigned char* f_;
+    const std::vector<Block>& blocks_;
+    std::vector<std::thread> threads_;
+    std::atomic<bool> bad_{false};
+    bool ok_ = true;
+};
+
 #define FCUDA(call)                                   \
     do {                                              \
         if ((call) != cudaSuccess) {                  \
@@ -60,9 +126,13 @@ struct Block {
 // (follows src/frame.cpp:53-278 for the statuses: any block reject is
 // CORRUPT_INPUT, the caller's capacity is checked before the first byte is
 // written, OUTPUT_TOO_SMALL otherwise).
+// `sums_ok` runs once the device results are in and before anything is
+// checked against the caller's capacity or copied to the caller: false (a
+// block checksum mismatch) is CORRUPT_INPUT with the output untouched, as
+// when the walk itself rejects the block.
 cudec_status decode_blocks(const unsigned char* f, const std::vector<Block>& blocks,
                            size_t block_max, unsigned char* out, size_t cap,
-                           size_t* total_out) {
+                           size_t* total_out, const std::function<bool()>& sums_ok) {
     std::vector<size_t> comp;
     for (size_t i = 0; i < blocks.size(); ++i)
         if (!blocks[i].raw) comp.push_back(i);
@@ -105,6 +175,7 @@ cudec_status decode_blocks(const unsigned char* f, const std::vector<Block>& blo
         FCUDA(cudaMemcpyAsync(res.data(), d_res.p, n * sizeof(cudec_chunk_result),
                               cudaMemcpyDeviceToHost, stream.s));
         FCUDA(cudaStreamSynchronize(stream.s));
+        if (!sums_ok()) return CUDEC_ERR_CORRUPT_INPUT;
         for (size_t k = 0; k < n; ++k) {
             // The per-block capacity is ours (block_max), never the caller's:
             // every block-level reject is a corrupt frame.
@@ -113,6 +184,7 @@ cudec_status decode_blocks(const unsigned char* f, const std::vector<Block>& blo
             dec_len[comp[k]] = static_cast<size_t>(res[k].bytes_written);
         }
     }
+    if (n == 0 && !sums_ok()) return CUDEC_ERR_CORRUPT_INPUT;
     size_t total = 0;
     for (size_t i = 0; i < blocks.size(); ++i) {
         const size_t len = blocks[i].raw ? blocks[i].len : dec_len[i];
@@ -191,17 +263,19 @@ cudec_status decode_frame(const unsigned char* f, size_t size, unsigned char* ou
         const bool raw = (bs >> 31) & 1;
         const size_t blen = bs & 0x7FFFFFFFu;
         if (blen == 0 || blen > block_max || size < pos + blen) return CUDEC_ERR_CORRUPT_INPUT;
-        if (block_sum) {
-            if (size < pos + blen + 4) return CUDEC_ERR_CORRUPT_INPUT;
-            if (xxh32(f + pos, blen) != rd32(f + pos + blen)) return CUDEC_ERR_CORRUPT_INPUT;
-        }
+        if (block_sum && size < pos + blen + 4) return CUDEC_ERR_CORRUPT_INPUT;
         blocks.push_back({pos, blen, raw});
         pos += blen + (block_sum ? 4 : 0);
     }
     if (!end) return CUDEC_ERR_CORRUPT_INPUT;
     size_t total = 0;
-    const cudec_status st = decode_blocks(f, blocks, block_max, out, cap, &total);
-    if (st != CUDEC_OK) return st;
+    // the checksum values are verified while the blocks decode
+    BlockSums sums(f, blocks, block_sum);
+    const cudec_status st =
+        decode_blocks(f, blocks, block_max, out, cap, &total, [&sums] { return sums.ok(); });
+    // a checksum mismatch outranks whatever the device path met (the walk
+    // would have stopped before any CUDA call)
+    if (st != CUDEC_OK) return sums.ok() ? st : CUDEC_ERR_CORRUPT_INPUT;
     if (has_size && declared != total) return CUDEC_ERR_CORRUPT_INPUT;
     if (content_sum) {
         if (size < pos + 4) return CUDEC_ERR_CORRUPT_INPUT;

@@ -138,6 +138,50 @@ def test_frame_entry_matches_oracle_and_reference(cuda):
             assert oracle.ref_lz4f_decode(body, cap)[0] == got[0], name
 
 
+def block_offsets(fr):
+    """(offset, length) of each block's data in an .lz4 frame with block
+    checksums (the 4-byte checksum follows each block)."""
+    flg = fr[4]
+    pos = 4 + 2 + (8 if flg & 8 else 0) + 1
+    out = []
+    while True:
+        bs = int.from_bytes(fr[pos:pos + 4], "little")
+        pos += 4
+        if bs == 0:
+            return out
+        n = bs & 0x7FFFFFFF
+        out.append((pos, n))
+        pos += n + 4
+
+
+@pytest.mark.gpu
+def test_frame_block_checksums_checked_in_parallel(cuda):
+    """Frames large enough for the block checksums to be verified on host
+    threads while the blocks decode: a good frame decodes; a bad checksum in
+    any block (first, middle, last, a stored block) is CORRUPT_INPUT, also
+    when the capacity is too small (the checksum outranks it), exactly as
+    the oracle's in-order walk decides."""
+    d = raw_data(12 << 20, seed=21)
+    noise = np.random.default_rng(2).integers(0, 256, 200000, dtype=np.uint8).tobytes()
+    d = d[:3 << 20] + noise + d[3 << 20:]  # an incompressible run: stored blocks
+    fr = W.lz4f_compress(d, block_size_id=4, content_checksum=True, block_checksum=True)
+    blocks = block_offsets(fr)
+    assert len(blocks) > 150
+    stored = [i for i, (o, n) in enumerate(blocks)
+              if int.from_bytes(fr[o - 4:o], "little") >> 31]
+    assert stored
+    st, out = cd.lz4f_decompress(fr, len(d))
+    assert st == 0 and out == d
+    for k in (0, len(blocks) // 2, len(blocks) - 1, stored[0]):
+        o, n = blocks[k]
+        g = bytearray(fr)
+        g[o + n] ^= 0x40  # the block's checksum
+        for cap in (len(d), len(d) - 1):
+            want = oracle.lz4f_decode(bytes(g), cap)
+            assert want[0] == cd.ERR_CORRUPT_INPUT
+            assert cd.lz4f_decompress(bytes(g), cap)[0] == want[0], (k, cap)
+
+
 def host_arrays(comps, caps, space, device=None):
     """Host pointer tables for the stream entry; destinations host or device."""
     import torch
