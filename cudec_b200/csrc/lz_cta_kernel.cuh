@@ -1145,7 +1145,9 @@ struct Chunk {
                 }
             }
 #ifdef CDB_PHASE_TIMING
-            atomicAdd(&lzc_events[6], static_cast<unsigned long long>(spin));
+            // one global add per warp (the counts summed across its lanes)
+            const unsigned ws = __reduce_add_sync(0xffffffffu, spin);
+            if ((t & 31) == 0) atomicAdd(&lzc_events[6], static_cast<unsigned long long>(ws));
 #endif
         });
 #else
