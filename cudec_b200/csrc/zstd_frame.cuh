@@ -134,7 +134,7 @@ __device__ __forceinline__ void lane_fill(uint8_t* dst, uint8_t b, uint64_t n) {
 }
 
 // One lane writes the match dst[ms, ms + n) at offset off (every byte before
-// ms is written; off is below the 8 MB window), 16 bytes at a time: the
+// ms is written; off is below the window, under 2^32), 16 bytes at a time: the
 // first piece is one read and one write in every lane (lzw::period16 for
 // periods under 16 bytes), the rest a plain copy at lzw::rest_distance(off).
 __device__ __forceinline__ void lane_match(uint8_t* dst, uint64_t ms, uint64_t n, uint64_t off) {
@@ -151,7 +151,11 @@ __device__ __forceinline__ void lane_match(uint8_t* dst, uint64_t ms, uint64_t n
 
 // Decode the frame at the start of f[0, N); every lane returns the same
 // status, *written and *consumed (the frame's bytes). Bytes after the frame
-// are not looked at.
+// are not looked at. Wide: the frame-sequence reading, which also takes a
+// frame without a content size (its output bounded by cap alone) and any
+// window whose log is at most kMaxWindowLogSeq; otherwise the reference's
+// subset.
+template <bool Wide>
 __device__ inline int decode_frame_part(const uint8_t* f, uint64_t N, uint8_t* dst, uint64_t cap,
                                         WarpSmem& w, uint8_t* litbuf, uint32_t lane,
                                         uint64_t* written, uint64_t* consumed) {
@@ -169,11 +173,12 @@ __device__ inline int decode_frame_part(const uint8_t* f, uint64_t N, uint8_t* d
     if (d & 3) return CUDEC_ERR_UNSUPPORTED;
     const unsigned fcs_size = fcs_flag == 0 ? (single ? 1 : 0)
                             : fcs_flag == 1 ? 2 : fcs_flag == 2 ? 4 : 8;
-    if (fcs_size == 0) return CUDEC_ERR_UNSUPPORTED;
+    const bool has_fcs = fcs_size != 0;  // single segment implies a content size
+    if (!has_fcs && !Wide) return CUDEC_ERR_UNSUPPORTED;
     const unsigned wbytes = single ? 0 : 1;
     const uint64_t hsz = 5 + wbytes + fcs_size;
     if (N < hsz) return CUDEC_ERR_CORRUPT_INPUT;
-    uint64_t fcs = rd_le(f + 5 + wbytes, fcs_size);
+    uint64_t fcs = has_fcs ? rd_le(f + 5 + wbytes, fcs_size) : 0;
     if (fcs_size == 2) fcs += 256;
     uint64_t window;
     if (single) {
@@ -181,9 +186,10 @@ __device__ inline int decode_frame_part(const uint8_t* f, uint64_t N, uint8_t* d
     } else {
         const uint64_t e = f[5] >> 3, m = f[5] & 7, base = 1ull << (10 + e);
         window = base + (base / 8) * m;
-        if (window > kMaxWindow) return CUDEC_ERR_UNSUPPORTED;
+        if (!Wide && window > kMaxWindow) return CUDEC_ERR_UNSUPPORTED;
+        if (Wide && 10 + e > kMaxWindowLogSeq) return CUDEC_ERR_UNSUPPORTED;
     }
-    if (fcs > cap) return CUDEC_ERR_OUTPUT_TOO_SMALL;
+    if (has_fcs && fcs > cap) return CUDEC_ERR_OUTPUT_TOO_SMALL;
     const uint64_t bmax = window < kLitSlot ? window : kLitSlot;
 
     Tables t;
@@ -194,7 +200,7 @@ __device__ inline int decode_frame_part(const uint8_t* f, uint64_t N, uint8_t* d
     }
     t.huf_log = 0;
     t.huf_present = false;
-    // repeat offsets stay below the window (at most 8 MB), so 32 bits
+    // repeat offsets stay below 2^32 (offset codes are at most 31), so 32 bits
     uint32_t rep0 = 1, rep1 = 4, rep2 = 8;
     uint64_t pos = hsz, out = 0;
     for (;;) {
@@ -565,7 +571,7 @@ __device__ inline int decode_frame_part(const uint8_t* f, uint64_t N, uint8_t* d
         pos += 3 + body;
         if (last) break;
     }
-    if (out != fcs) return CUDEC_ERR_CORRUPT_INPUT;
+    if (has_fcs && out != fcs) return CUDEC_ERR_CORRUPT_INPUT;
     if (csum) {
         if (N - pos < 4) return CUDEC_ERR_CORRUPT_INPUT;
         __syncwarp();
@@ -589,7 +595,7 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
                                    uint64_t* written) {
     uint64_t out = 0, used = 0;
     *written = 0;
-    const int st = decode_frame_part(f, N, dst, cap, w, litbuf, lane, &out, &used);
+    const int st = decode_frame_part<false>(f, N, dst, cap, w, litbuf, lane, &out, &used);
     if (st != CUDEC_OK) return st;
     if (used != N) return CUDEC_ERR_CORRUPT_INPUT;
     *written = out;
@@ -597,11 +603,14 @@ __device__ inline int decode_frame(const uint8_t* f, uint64_t N, uint8_t* dst, u
 }
 
 // A chunk of concatenated frames, as libzstd's ZSTD_decompress reads a
-// buffer (the first rung of the reference's subset ladder,
-// docs/MASTERPLAN.md:1286-1289): skippable frames (magic 0x184D2A50-5F,
-// 4-byte size) are skipped, each Zstd frame (in the v1 subset above)
-// decodes after the previous one's output; fewer than 4 bytes left, or a
-// skippable frame running past the chunk, is CORRUPT_INPUT.
+// buffer with its default limits (the reference's subset ladder,
+// docs/MASTERPLAN.md:1286-1296, rungs 1-3 up to that limit): skippable
+// frames (magic 0x184D2A50-5F, 4-byte size) are skipped, and each Zstd frame
+// decodes after the previous one's output, with or without a content size,
+// with any window up to a log of kMaxWindowLogSeq (a dictionary id stays
+// UNSUPPORTED);
+// fewer than 4 bytes left, or a skippable frame running past the chunk, is
+// CORRUPT_INPUT.
 __device__ inline int decode_frames(const uint8_t* f, uint64_t N, uint8_t* dst, uint64_t cap,
                                     WarpSmem& w, uint8_t* litbuf, uint32_t lane,
                                     uint64_t* written) {
@@ -618,8 +627,8 @@ __device__ inline int decode_frames(const uint8_t* f, uint64_t N, uint8_t* dst, 
             continue;
         }
         uint64_t fo = 0, used = 0;
-        const int st = decode_frame_part(f + pos, N - pos, dst + out, cap - out, w, litbuf, lane,
-                                         &fo, &used);
+        const int st = decode_frame_part<true>(f + pos, N - pos, dst + out, cap - out, w,
+                                               litbuf, lane, &fo, &used);
         if (st != CUDEC_OK) return st;
         out += fo;
         pos += used;

@@ -43,6 +43,11 @@ constexpr int kWarpsPerCta = 4;
 constexpr int kCtaThreads = kWarpsPerCta * 32;
 constexpr uint32_t kLitSlot = 128 * 1024;   // per-warp literal buffer (block maximum)
 constexpr uint64_t kMaxWindow = 8ull << 20;
+// Frame sequences (decode_frames): the largest window log libzstd's
+// one-shot decoder takes (ZSTD_WINDOWLOG_MAX on 64-bit hosts). The window
+// costs nothing here (matches read the destination), and offsets stay below
+// 2^32 (an offset code is at most 31).
+constexpr uint32_t kMaxWindowLogSeq = 31;
 
 constexpr uint32_t kFseCells = 512;  // FSE decode cells per field (table log <= 9)
 

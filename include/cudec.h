@@ -138,19 +138,22 @@ cudec_status cudec_zstd_decompress_batch(const void* const* d_src_ptrs,
                                          size_t workspace_bytes,
                                          cudec_stream_t stream);
 
-/* Zstd chunks that hold a sequence of frames, the first rung of the
- * reference's subset ladder (docs/MASTERPLAN.md:1286-1289), which the
- * reference leaves untaken; no counterpart in its ABI. A chunk is read the
- * way libzstd's ZSTD_decompress reads a buffer: skippable frames (magic
+/* Zstd chunks that hold a sequence of frames, read the way libzstd's
+ * one-shot ZSTD_decompress reads a buffer: the reference's subset ladder
+ * (docs/MASTERPLAN.md:1286-1296), which the reference leaves untaken, up to
+ * that decoder's limits; no counterpart in its ABI. Skippable frames (magic
  * 0x184D2A50-0x184D2A5F, then a 4-byte little-endian size) are skipped, and
- * each Zstd frame, in the same v1 subset as cudec_zstd_decompress_batch,
- * decodes into the output right after the previous frame's bytes. The chunk
- * keeps one 16-byte record: bytes_written is the sum over its frames, and
- * the status is the first failing frame's (then bytes_written is 0 and the
- * output is undefined). An empty chunk decodes to zero bytes; fewer than 4
- * bytes left after a frame, or a skippable frame that runs past the chunk,
- * is CUDEC_ERR_CORRUPT_INPUT. Workspace and every argument rule as
- * cudec_zstd_decompress_batch; the one-frame entry above is unchanged. */
+ * each Zstd frame decodes into the output right after the previous frame's
+ * bytes. Beyond cudec_zstd_decompress_batch's subset a frame may omit its
+ * content size (its output is bounded by the capacity alone) and may declare
+ * any window up to a window log of 31; a dictionary id, or a larger window
+ * log, is CUDEC_ERR_UNSUPPORTED. The chunk keeps one 16-byte record:
+ * bytes_written is the sum over its frames, and the status is the first
+ * failing frame's (then bytes_written is 0 and the output is undefined). An
+ * empty chunk decodes to zero bytes; fewer than 4 bytes left after a frame,
+ * or a skippable frame that runs past the chunk, is CUDEC_ERR_CORRUPT_INPUT.
+ * Workspace and every argument rule as cudec_zstd_decompress_batch; the
+ * one-frame entry above is unchanged. */
 cudec_status cudec_zstd_decompress_batch_multi(const void* const* d_src_ptrs,
                                                const size_t* d_src_sizes,
                                                void* const* d_dst_ptrs,

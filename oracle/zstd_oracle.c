@@ -612,9 +612,12 @@ static int z_repcode(uint64_t* rep, uint64_t ov, uint32_t ll, uint64_t* out) {
 }
 
 /* One frame at the start of f[0, n); *consumed is its length in bytes and
- * bytes after it are not looked at. */
+ * bytes after it are not looked at. wide: the frame-sequence reading, which
+ * also takes a frame without a content size (output bounded by cap) and any
+ * window whose log is at most 31 (libzstd's one-shot limit, ZSTD_WINDOWLOG_MAX
+ * on 64-bit hosts). */
 static int z_frame(const uint8_t* f, uint64_t n, uint8_t* dst, uint64_t cap,
-                   uint64_t* written, uint64_t* consumed) {
+                   uint64_t* written, uint64_t* consumed, int wide) {
     *written = 0;
     *consumed = 0;
     if (n < 4) return Z_CORRUPT;
@@ -629,11 +632,12 @@ static int z_frame(const uint8_t* f, uint64_t n, uint8_t* dst, uint64_t cap,
     if (d & 8) return Z_CORRUPT;
     if (did) return Z_UNSUPPORTED;
     const unsigned fcs_size = fcs_flag == 0 ? (single ? 1 : 0) : fcs_flag == 1 ? 2 : fcs_flag == 2 ? 4 : 8;
-    if (fcs_size == 0) return Z_UNSUPPORTED;
+    const int has_fcs = fcs_size != 0; /* single segment implies a content size */
+    if (!has_fcs && !wide) return Z_UNSUPPORTED;
     const unsigned wbytes = single ? 0 : 1;
     const uint64_t hsz = 5 + wbytes + fcs_size;
     if (n < hsz) return Z_CORRUPT;
-    uint64_t fcs = z_le(f + 5 + wbytes, fcs_size);
+    uint64_t fcs = has_fcs ? z_le(f + 5 + wbytes, fcs_size) : 0;
     if (fcs_size == 2) fcs += 256;
     uint64_t window;
     if (single) {
@@ -641,9 +645,10 @@ static int z_frame(const uint8_t* f, uint64_t n, uint8_t* dst, uint64_t cap,
     } else {
         const uint64_t e = f[5] >> 3, m = f[5] & 7, base = 1ull << (10 + e);
         window = base + (base / 8) * m;
-        if (window > (8ull << 20)) return Z_UNSUPPORTED;
+        if (!wide && window > (8ull << 20)) return Z_UNSUPPORTED;
+        if (wide && 10 + e > 31) return Z_UNSUPPORTED;
     }
-    if (fcs > cap) return Z_TOO_SMALL;
+    if (has_fcs && fcs > cap) return Z_TOO_SMALL;
 
     zstate* z = (zstate*)calloc(1, sizeof(zstate));
     const uint64_t bmax = window < 131072 ? window : 131072;
@@ -777,7 +782,7 @@ static int z_frame(const uint8_t* f, uint64_t n, uint8_t* dst, uint64_t cap,
         pos += 3 + body;
         if (last) break;
     }
-    if (out != fcs) { st = Z_CORRUPT; goto done; }
+    if (has_fcs && out != fcs) { st = Z_CORRUPT; goto done; }
     if (csum) {
         if (n - pos < 4) { st = Z_CORRUPT; goto done; }
         if ((uint32_t)oracle_xxh64(dst, out, 0) != (uint32_t)z_le(f + pos, 4)) {
@@ -800,18 +805,20 @@ int oracle_zstd_decode(const uint8_t* f, uint64_t n, uint8_t* dst, uint64_t cap,
                        uint64_t* written) {
     uint64_t out = 0, used = 0;
     *written = 0;
-    const int st = z_frame(f, n, dst, cap, &out, &used);
+    const int st = z_frame(f, n, dst, cap, &out, &used, 0);
     if (st != Z_OK) return st;
     if (used != n) return Z_CORRUPT;
     *written = out;
     return Z_OK;
 }
 
-/* Concatenated frames as libzstd's ZSTD_decompress reads them (the first
- * rung of the reference's subset ladder, docs/MASTERPLAN.md:1286-1289):
- * skippable frames (magic 0x184D2A50-5F, 4-byte little-endian size) are
- * skipped, each Zstd frame decodes after the previous one's output; fewer
- * than 4 bytes left, or a skippable frame past the end, is CORRUPT. */
+/* Concatenated frames as libzstd's ZSTD_decompress reads them with its
+ * default limits (the reference's subset ladder, docs/MASTERPLAN.md:
+ * 1286-1296, rungs 1-3 up to that limit): skippable frames (magic
+ * 0x184D2A50-5F, 4-byte little-endian size) are skipped, each Zstd frame
+ * decodes after the previous one's output, with or without a content size,
+ * with any window up to a log of 31 (a dictionary id stays UNSUPPORTED);
+ * fewer than 4 bytes left, or a skippable frame past the end, is CORRUPT. */
 int oracle_zstd_decode_multi(const uint8_t* f, uint64_t n, uint8_t* dst, uint64_t cap,
                              uint64_t* written) {
     uint64_t pos = 0, out = 0;
@@ -827,7 +834,7 @@ int oracle_zstd_decode_multi(const uint8_t* f, uint64_t n, uint8_t* dst, uint64_
             continue;
         }
         uint64_t fo = 0, used = 0;
-        const int st = z_frame(f + pos, n - pos, dst + out, cap - out, &fo, &used);
+        const int st = z_frame(f + pos, n - pos, dst + out, cap - out, &fo, &used, 1);
         if (st != Z_OK) return st;
         out += fo;
         pos += used;

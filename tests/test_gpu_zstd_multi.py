@@ -4,8 +4,9 @@ oracle's multi-frame reading (oracle_zstd_decode_multi, itself pinned to
 libzstd's ZSTD_decompress): frame sequences at exact, short and generous
 capacities, the edge cases around one frame, unaligned buffers, subset
 refusals inside a sequence, mutated sequences, and the one-frame entry left
-strict on the same chunks. Destinations are poisoned; nothing past
-bytes_written may change."""
+strict on the same chunks; frames without a content size and windows
+above 8 MB, which this entry takes as libzstd's one-shot decoder does.
+Destinations are poisoned; nothing past bytes_written may change."""
 import json
 import os
 import random
@@ -93,17 +94,39 @@ def test_unaligned_buffers(cuda, skew):
     assert all(int(s) == 0 for s in res["status"])
 
 
-def test_subset_refusals_inside_a_sequence(cuda):
+def test_wider_subset(cuda):
+    """Beyond the reference's subset, as libzstd's one-shot decoder: frames
+    without a content size (levels 1/3/19, with and without checksums, alone
+    and in sequences), a 16 MiB window, window logs at and past 31; the
+    reference's other refusals next to a decodable frame. Device equals the
+    oracle; the one-frame entry still refuses them."""
     import zstd_subset
     raw = corpus([2000], seed=67)[0]
     f = W.zstd_compress(raw, 3, 20, False)
     cases = zstd_subset.refused_frames()
     comps = [f + c[0] for c in cases.values()] + [c[0] + f for c in cases.values()]
     caps = [len(raw) + c[1] for c in cases.values()] * 2
+    for r in corpus([1, 777, 70000, 300000], seed=69):
+        for lvl in (1, 3, 19):
+            for ck in (False, True):
+                g = W.zstd_compress(r, lvl, 20, ck, content_size=False)
+                comps += [g, g + f, g]
+                caps += [len(r), len(r) + len(raw), max(len(r) - 1, 0)]
+    big = corpus([12 << 20], seed=71)[0]
+    comps.append(W.zstd_compress(big, 3, 24, True, content_size=False))
+    caps.append(len(big))
+    magic = b"\x28\xb5\x2f\xfd"
+    for exp in (18, 21, 22, 31):
+        comps.append(magic + bytes([0x00, exp << 3]) + b"\x01\x00\x00")
+        caps.append(64)
     b, res, dst = run_batch(cuda, comps, caps)
-    check(b, res, dst, comps, caps, "subset")
-    want = [0 if name == "skippable" else 6 for name in cases]
-    assert [int(s) for s in res["status"]] == want * 2
+    check(b, res, dst, comps, caps, "wide")
+    sts = [int(x) for x in res["status"]]
+    want = [6 if name == "dictionary id" else 0 for name in cases]
+    assert sts[:2 * len(cases)] == want * 2
+    assert sts[-5:] == [0, 0, 0, 6, 6]
+    b1, r1, _ = run_batch(cuda, comps, caps, fmt="zstd")
+    assert all(int(x) != 0 for x in r1["status"][2 * len(cases):])
 
 
 def test_mutated_sequences(cuda):

@@ -1,10 +1,11 @@
 """Pins the multi-frame Zstd oracle (oracle_zstd_decode_multi in
 oracle/zstd_oracle.c) against libzstd's ZSTD_decompress, which reads a
 buffer as a sequence of Zstd and skippable frames: the same bytes on every
-accepted sequence, the same refusals on truncated sequences and trailing
-bytes, and never an accept where libzstd refuses. The one-frame oracle (the
-reference's rule, pinned in test_zstd_oracle.py) stays strict on the same
-inputs."""
+accepted sequence (frames without a content size and windows above 8 MB
+included), the same refusals on truncated sequences, trailing bytes and
+windows past libzstd's default limit, and never an accept where libzstd
+refuses. The one-frame oracle (the reference's rule, pinned in
+test_zstd_oracle.py) stays strict on the same inputs."""
 import random
 
 import numpy as np
@@ -61,18 +62,51 @@ def test_edges_match_libzstd():
             assert ref is None, name
 
 
-def test_subset_refusals_inside_a_sequence():
-    """A frame outside the subset stays UNSUPPORTED wherever it sits in the
-    chunk; a skippable frame is no longer a refusal."""
+def test_wider_subset_matches_libzstd():
+    """The frame-sequence reading takes what libzstd's one-shot decoder takes
+    beyond the reference's subset: frames without a content size and windows
+    above 8 MB (any window log up to 31); a dictionary id stays UNSUPPORTED
+    and a window log above 31 is refused as libzstd refuses it. The one-frame
+    reading still refuses all of them."""
     import zstd_subset
     raw = corpus([2000], seed=31)[0]
     f = W.zstd_compress(raw, 3, 20, False)
-    for name, (frame, cap, _) in zstd_subset.refused_frames().items():
+    for name, (frame, cap, libzstd_ok) in zstd_subset.refused_frames().items():
         got = oracle.zstd_decode_multi(f + frame, len(raw) + cap)
-        if name == "skippable":
-            assert got == (OK, raw), name
-        else:
+        assert oracle.zstd_decode(frame, cap)[0] == UNSUPPORTED, name
+        if name == "dictionary id":
             assert got == (UNSUPPORTED, b""), name
+        else:
+            assert libzstd_ok, name
+            want = W.zstd_decompress_ref(f + frame, len(raw) + cap)
+            assert got == (OK, want), name
+    # no content size, levels and checksums, alone and in sequences
+    for r in corpus([1, 777, 70000, 300000], seed=33):
+        for lvl in (1, 3, 19):
+            for ck in (False, True):
+                g = W.zstd_compress(r, lvl, 20, ck, content_size=False)
+                assert g[4] >> 6 == 0 and not g[4] & 0x20  # no content size field
+                assert oracle.zstd_decode(g, len(r))[0] == UNSUPPORTED
+                assert oracle.zstd_decode_multi(g, len(r)) == (OK, r)
+                assert oracle.zstd_decode_multi(g + f, len(r) + len(raw)) == (OK, r + raw)
+                if r:
+                    assert oracle.zstd_decode_multi(g, len(r) - 1)[0] == TOO_SMALL
+    # a 16 MiB window (content larger than 8 MiB, no content size)
+    big = corpus([12 << 20], seed=35, rle=0.05)[0]
+    g = W.zstd_compress(big, 3, 24, True, content_size=False)
+    wd = g[5]
+    assert (1 << (10 + (wd >> 3))) > (8 << 20)
+    assert oracle.zstd_decode(g, len(big))[0] == UNSUPPORTED
+    assert oracle.zstd_decode_multi(g, len(big)) == (OK, big)
+    assert W.zstd_decompress_ref(g, len(big)) == big
+    # empty frames (one empty last raw block) by window log: up to 31 both
+    # decode, above it both refuse
+    magic = b"\x28\xb5\x2f\xfd"
+    for exp, mant in ((14, 0), (18, 7), (21, 7), (22, 0), (31, 7)):
+        fr = magic + bytes([0x00, (exp << 3) | mant]) + b"\x01\x00\x00"
+        ok = 10 + exp <= 31
+        assert oracle.zstd_decode_multi(fr, 64) == ((OK, b"") if ok else (UNSUPPORTED, b"")), exp
+        assert (W.zstd_decompress_ref(fr, 64) == b"") == ok, exp
 
 
 def test_mutated_sequences_never_accept_what_libzstd_refuses():
