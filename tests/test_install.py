@@ -53,9 +53,10 @@ def test_installed_files(prefix):
                 "lib/cmake/cudec/cudec-config-version.cmake", "lib/pkgconfig/cudec.pc"):
         assert os.path.isfile(os.path.join(prefix, rel)), rel
     assert "Version: " + ver in open(os.path.join(prefix, "lib/pkgconfig/cudec.pc")).read()
-    soname = subprocess.run(["readelf", "-d", os.path.join(prefix, "lib/libcudec_b200.so")],
-                            capture_output=True, text=True).stdout
-    assert "[libcudec_b200.so]" in soname
+    if shutil.which("readelf"):
+        soname = subprocess.run(["readelf", "-d", os.path.join(prefix, "lib/libcudec_b200.so")],
+                                capture_output=True, text=True).stdout
+        assert "[libcudec_b200.so]" in soname
 
 
 @pytest.mark.skipif(CMAKE is None, reason="cmake not installed")
