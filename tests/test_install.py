@@ -4,8 +4,9 @@ gives a prefix that a CMake consumer finds with find_package(cudec) and links
 through the imported target cudec::cudec, and that pkg-config describes. The
 consumer here is the C conformance program (tests/conformance_c.c, C99),
 built against the installed header and library only and run (its checks need
-no GPU). Version requests follow the 0.x rule (same major.minor, patch at or
-below), and the prefix still works after it is moved."""
+no GPU). Version requests follow the 0.x rule (met by the same major.minor
+at an installed patch level at or above the one requested), and the prefix
+still works after it is moved."""
 import os
 import shutil
 import subprocess
