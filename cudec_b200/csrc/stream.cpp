@@ -16,8 +16,10 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "cudec.h"
@@ -145,9 +147,14 @@ namespace {
 // exactly bytes_written per chunk, bounded by the chunk's capacity (a longer
 // device-reported length is a device fault: the chunk is stamped CUDA and
 // the wave fails, as src/stream.cpp:163-184 does).
+// Every record is checked before any byte moves; the copies of a wave of
+// kParallelScatter bytes or more are split into chunk ranges of about equal
+// bytes over up to 16 host threads (the calling thread takes one range).
+constexpr size_t kParallelScatter = size_t{4} << 20;
+
 cudec_status scatter_wave(cudec_chunk_result* wr, const unsigned char* staged,
                           void* const* dst, const size_t* caps, size_t begin, size_t wn) {
-    size_t off = 0;
+    size_t total = 0;
     for (size_t j = 0; j < wn; ++j) {
         const size_t i = begin + j;
         const size_t bw = static_cast<size_t>(wr[j].bytes_written);
@@ -157,9 +164,46 @@ cudec_status scatter_wave(cudec_chunk_result* wr, const unsigned char* staged,
             wr[j].bytes_written = 0;
             return CUDEC_ERR_CUDA;
         }
-        if (bw != 0 && dst[i] != nullptr) std::memcpy(dst[i], staged + off, bw);
-        off += caps[i];
+        total += bw;
     }
+    // chunks [j0, j1) from staging offset off0
+    auto copy = [&](size_t j0, size_t j1, size_t off0) {
+        size_t off = off0;
+        for (size_t j = j0; j < j1; ++j) {
+            const size_t i = begin + j;
+            const size_t bw = static_cast<size_t>(wr[j].bytes_written);
+            if (bw != 0 && dst[i] != nullptr) std::memcpy(dst[i], staged + off, bw);
+            off += caps[i];
+        }
+    };
+    const unsigned hw = std::thread::hardware_concurrency();
+    const size_t nt = std::min<size_t>({hw ? hw : 1u, 16u, wn});
+    if (total < kParallelScatter || nt < 2) {
+        copy(0, wn, 0);
+        return CUDEC_OK;
+    }
+    // range boundaries at about total / nt decoded bytes each
+    std::vector<size_t> jb(1, 0), ob(1, 0);
+    size_t acc = 0, off = 0;
+    for (size_t j = 0; j < wn; ++j) {
+        acc += static_cast<size_t>(wr[j].bytes_written);
+        off += caps[begin + j];
+        if (jb.size() < nt && acc >= total / nt * jb.size() && j + 1 < wn) {
+            jb.push_back(j + 1);
+            ob.push_back(off);
+        }
+    }
+    jb.push_back(wn);
+    std::vector<std::thread> threads;
+    size_t r = 1;
+    try {
+        for (; r + 1 < jb.size(); ++r)
+            threads.emplace_back(copy, jb[r], jb[r + 1], ob[r]);
+    } catch (...) {  // no thread to be had: the rest on this one
+        for (; r + 1 < jb.size(); ++r) copy(jb[r], jb[r + 1], ob[r]);
+    }
+    copy(jb[0], jb[1], ob[0]);
+    for (std::thread& th : threads) th.join();
     return CUDEC_OK;
 }
 

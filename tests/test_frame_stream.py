@@ -262,6 +262,43 @@ def test_stream_many_waves_and_one_shot(cuda):
 
 
 @pytest.mark.gpu
+def test_stream_host_output_large_waves(cuda):
+    """Host output in waves large enough for the copy to the caller's
+    buffers to be split over host threads (uneven chunk sizes, some corrupt
+    chunks and capacities too small among them): every chunk's bytes and
+    record equal the oracle's, exactly bytes_written bytes land, the rest of
+    each destination keeps its fill, and the aggregate is the first non-OK
+    chunk in index order."""
+    rng = random.Random(31)
+    n = 700
+    raws = [raw_data(rng.choice([100, 5000, 65536, 200000]), seed=500 + i) for i in range(n)]
+    comps = [W.lz4_compress(r) for r in raws]
+    caps = [len(r) + rng.choice([0, 0, 0, 7]) for r in raws]
+    for i in rng.sample(range(n), 12):  # corrupt a few: a bad offset, or a capacity too small
+        if i % 2:
+            caps[i] = max(len(raws[i]) - 1, 0)
+        else:
+            c = bytearray(comps[i])
+            c[len(c) // 2] ^= 0xFF
+            comps[i] = bytes(c)
+    ctx = cd.StreamContext()
+    st, res, outs = run_stream(ctx, comps, caps, cd.MEM_HOST)
+    first = None
+    for i in range(n):
+        want_st, want = oracle.lz4_decode(comps[i], caps[i])
+        assert int(res[i]["status"]) == want_st, i
+        if want_st == 0:
+            assert int(res[i]["bytes_written"]) == len(want)
+            assert outs[i][:len(want)] == want, i
+            assert outs[i][len(want):] == bytes([0xA5]) * (len(outs[i]) - len(want)), i
+        else:
+            assert int(res[i]["bytes_written"]) == 0
+            first = i if first is None else first
+    assert first is not None and st == int(res[first]["status"])
+    ctx.close()
+
+
+@pytest.mark.gpu
 def test_stream_poison_latch_on_allocation_failure(cuda):
     """An impossible host-output staging size makes the grow allocation fail
     on the host side: CUDA status, every record defined, context poisoned,
