@@ -262,6 +262,16 @@ cudec_status decode(cudec_stream_ctx& ctx, const void* const* src, const size_t*
     cudec_chunk_result* p_res = static_cast<cudec_chunk_result*>(ctx.p_results.p);
     stamp(p_res, n, CUDEC_ERR_CUDA);
 
+    // Host output in one wave to destinations that sit back to back in index
+    // order (one caller buffer): once every chunk is known to have filled
+    // its capacity, the decoded wave goes to the caller in one copy, with no
+    // staging pass; otherwise it takes the staged path below.
+    bool direct = host_out && waves == 1 && dst[0] != nullptr;
+    for (size_t i = 1; i < n && direct; ++i)
+        if (static_cast<unsigned char*>(dst[i]) !=
+            static_cast<unsigned char*>(dst[i - 1]) + caps[i - 1])
+            direct = false;
+
     cudec_status fail = CUDEC_OK;
     bool slot_busy[2] = {false, false};
     size_t slot_begin[2] = {0, 0}, slot_n[2] = {0, 0};
@@ -337,7 +347,7 @@ cudec_status decode(cudec_stream_ctx& ctx, const void* const* src, const size_t*
             fail = CUDEC_ERR_CUDA;
             break;
         }
-        if (host_out && oo &&
+        if (host_out && oo && !direct &&
             cudaMemcpyAsync(ctx.p_out[b].p, dout, oo, cudaMemcpyDeviceToHost, s) != cudaSuccess) {
             fail = CUDEC_ERR_CUDA;
             break;
@@ -354,6 +364,23 @@ cudec_status decode(cudec_stream_ctx& ctx, const void* const* src, const size_t*
     cudec_status drain = fail;
     if (cudaStreamSynchronize(s) != cudaSuccess && drain == CUDEC_OK) drain = CUDEC_ERR_CUDA;
     if (cudaGetLastError() != cudaSuccess && drain == CUDEC_OK) drain = CUDEC_ERR_CUDA;
+    if (drain == CUDEC_OK && direct && slot_busy[0]) {
+        // the records are in: every chunk full means one copy to the caller
+        size_t total = 0;
+        bool full = true;
+        for (size_t i = 0; i < n; ++i) {
+            full = full && p_res[i].status == CUDEC_OK &&
+                   static_cast<size_t>(p_res[i].bytes_written) == caps[i];
+            total += caps[i];
+        }
+        const void* dout = ctx.d_out[0].p;
+        void* to = full ? dst[0] : ctx.p_out[0].p;
+        if (total && (cudaMemcpyAsync(to, dout, total, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                      cudaStreamSynchronize(s) != cudaSuccess))
+            drain = CUDEC_ERR_CUDA;
+        else if (full)
+            slot_busy[0] = false;  // delivered; otherwise scattered from staging below
+    }
     if (drain == CUDEC_OK) {
         // finish in wave order (the older slot first)
         const int first = waves > 1 ? static_cast<int>((waves - 2) & 1) : 0;

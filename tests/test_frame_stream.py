@@ -299,6 +299,51 @@ def test_stream_host_output_large_waves(cuda):
 
 
 @pytest.mark.gpu
+def test_stream_host_output_one_buffer(cuda):
+    """Destinations back to back in one host buffer (the shape that lets a
+    full wave go to the caller in one copy): every chunk full; then one chunk
+    with spare capacity and one corrupt chunk, which take the staged path.
+    Bytes and records equal the oracle's, and nothing past bytes_written
+    changes."""
+    n = 300
+    raws = [raw_data(20000 + 37 * i, seed=900 + i) for i in range(n)]
+    base_comps = [W.lz4_compress(r) for r in raws]
+    for case in ("full", "mixed"):
+        comps = list(base_comps)
+        caps = [len(r) for r in raws]
+        if case == "mixed":
+            caps[17] += 9
+            c = bytearray(comps[200])
+            c[len(c) // 2] ^= 0xFF
+            comps[200] = bytes(c)
+        offs = np.concatenate([[0], np.cumsum(caps)]).astype(np.int64)
+        buf = np.full(int(offs[-1]), 0xA5, dtype=np.uint8)
+        srcs = [np.frombuffer(c, dtype=np.uint8).copy() for c in comps]
+        sp = np.array([x.ctypes.data for x in srcs], dtype=np.uint64)
+        sz = np.array([len(c) for c in comps], dtype=np.uint64)
+        cp = np.array(caps, dtype=np.uint64)
+        dp = np.array([buf.ctypes.data + int(o) for o in offs[:-1]], dtype=np.uint64)
+        res = np.zeros(n, dtype=[("status", "<i4"), ("reserved", "<u4"), ("bytes_written", "<u8")])
+        ctx = cd.StreamContext()
+        st = ctx.decode(sp.ctypes.data, sz.ctypes.data, dp.ctypes.data, cp.ctypes.data, n,
+                        cd.MEM_HOST, res.ctypes.data)
+        ctx.close()
+        first = None
+        for i in range(n):
+            want_st, want = oracle.lz4_decode(comps[i], caps[i])
+            assert int(res[i]["status"]) == want_st, (case, i)
+            seg = buf[offs[i]:offs[i + 1]].tobytes()
+            if want_st == 0:
+                assert seg[:len(want)] == want, (case, i)
+                assert seg[len(want):] == bytes([0xA5]) * (len(seg) - len(want)), (case, i)
+            else:
+                assert seg == bytes([0xA5]) * len(seg), (case, i)
+                first = i if first is None else first
+        assert st == (0 if first is None else int(res[first]["status"])), case
+        assert (first is None) == (case == "full")
+
+
+@pytest.mark.gpu
 def test_stream_poison_latch_on_allocation_failure(cuda):
     """An impossible host-output staging size makes the grow allocation fail
     on the host side: CUDA status, every record defined, context poisoned,
