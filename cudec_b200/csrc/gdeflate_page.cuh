@@ -373,12 +373,14 @@ __device__ __forceinline__ int decode_page(const uint8_t* pg, uint64_t N, uint8_
             const bool want_lit = !pend && !eob;
             uint32_t sym = 0, clen = 0;
             bool valid = true;
-            if (want_dist)
-                valid = decode_sym(ln.bb, sm.dtab, sm.dcount, sm.dsym, sm.dfirst, sm.dindex, &sym,
-                                   &clen);
-            else if (want_lit)
-                valid = decode_sym(ln.bb, sm.ltab, sm.lcount, sm.lsym, sm.lfirst, sm.lindex, &sym,
-                                   &clen);
+            // one decode for both kinds of lane (the code chosen per lane),
+            // so the warp does not run the two in turn
+            if (want_dist || want_lit) {
+                const bool dd = want_dist;
+                valid = decode_sym(ln.bb, dd ? sm.dtab : sm.ltab, dd ? sm.dcount : sm.lcount,
+                                   dd ? sm.dsym : sm.lsym, dd ? sm.dfirst : sm.lfirst,
+                                   dd ? sm.dindex : sm.lindex, &sym, &clen);
+            }
             const unsigned eobm = __ballot_sync(0xffffffffu, want_lit && valid && sym == 256);
             const uint32_t e = eobm ? __ffs(eobm) - 1 : 32;
             // a bad code stops the round at its lane if that lane would act:
