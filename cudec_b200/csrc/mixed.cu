@@ -256,12 +256,12 @@ __global__ void __launch_bounds__(kThreads, 2) mixed_kernel(Args a) {
     }
 }
 
-// Warps per LZ4 / Snappy chunk by bucket when the plan is created: a whole
-// CTA in every bucket (measured on B200 over 100,000 uneven LZ4 + Snappy
-// chunks: the CTA decoder's parallel parse beats one warp's serial chain
-// from the smallest bucket up); Zstd and GDeflate chunks are one warp's.
-constexpr uint32_t kDefaultWpc[kBuckets] = {kCtaWarps, kCtaWarps, kCtaWarps,
-                                            kCtaWarps, kCtaWarps, kCtaWarps};
+// Warps per LZ4 / Snappy chunk by bucket when the plan is created: one warp
+// below 16 KiB, a whole CTA from 16 KiB up (what the tuner picks on B200
+// over 100,000 uneven LZ4 + Snappy chunks, run after run: small chunks keep
+// the warp grid busy beside the CTA grid, and the CTA decoder's parallel
+// parse wins from 16 KiB up); Zstd and GDeflate chunks are one warp's.
+constexpr uint32_t kDefaultWpc[kBuckets] = {1, 1, kCtaWarps, kCtaWarps, kCtaWarps, kCtaWarps};
 
 struct Key {
     const void* const* src;

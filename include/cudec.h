@@ -282,8 +282,9 @@ cudec_status cudec_mixed_plan_get_tuning(const cudec_mixed_plan* plan,
 /* The whole decode shape, 4 values per bucket b: out_shape[4*b] = warps per
  * LZ4 / Snappy chunk (1: one warp; CUDEC_MIXED_CTA_WARPS: a whole CTA runs
  * the CTA-per-chunk decoder), then parse reach, lookahead and ring batch of
- * the one-warp decoder. A plan starts from a compiled-in table (a CTA per
- * LZ4 / Snappy chunk in every bucket); cudec_mixed_plan_tune measures one on
+ * the one-warp decoder. A plan starts from a compiled-in table (one warp per
+ * LZ4 / Snappy chunk below 16 KiB, a whole CTA from 16 KiB up);
+ * cudec_mixed_plan_tune measures one on
  * the caller's chunks. A caller can save the shape and set it on later
  * plans, so the decode shape is fixed across runs; set_shape refuses
  * (INVALID_ARGUMENT, nothing changed) a warps value other than 1 or

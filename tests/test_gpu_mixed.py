@@ -127,7 +127,7 @@ def test_warps_per_chunk_shapes_agree(cuda):
     recs, outs = per_format(cuda, comps, caps, fmts)
     plan = cd.MixedPlan()
     default = plan.shape()
-    assert [s[0] for s in default] == [cd.MIXED_CTA_WARPS] * 6
+    assert [s[0] for s in default] == [1, 1] + [cd.MIXED_CTA_WARPS] * 4
     b = DeviceBatch(comps, caps, device=cuda)
     for wpc in (1, cd.MIXED_CTA_WARPS, None):
         shape = default if wpc is None else [(wpc,) + tuple(s[1:]) for s in default]
