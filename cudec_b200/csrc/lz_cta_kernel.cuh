@@ -452,6 +452,36 @@ struct SnappyF : lzl::SnappyLadder {
 };
 
 // ---------------------------------------------------------------------------
+// The tile's token records. LZ4: 32-bit fields, a token's position reused
+// during execution for the in-group part of its match source. Snappy (up to
+// kTile / 2 tokens a tile): 16-bit positions and lengths (lengths saturate:
+// a longer token is a whole-CTA token, re-read by the ladder) and the
+// in-group sources in their own array, so that four CTAs share an SM.
+template <class F, bool Narrow = F::kSnappy>
+struct TokRecs;
+template <class F>
+struct TokRecs<F, false> {
+    static constexpr uint64_t kSat = 0xFFFFFFFFull;
+    uint32_t pos[F::kMaxTok];  // token position - e; executing: its match's in-group source
+    uint32_t lit[F::kMaxTok];  // saturated at kSat
+    uint32_t ml[F::kMaxTok];
+    uint32_t off[F::kMaxTok];
+    uint32_t out[F::kMaxTok];  // output offset - d0
+    CDB_HD uint32_t& dep(uint32_t i, uint32_t) { return pos[i]; }
+};
+template <class F>
+struct TokRecs<F, true> {
+    static constexpr uint64_t kSat = 0xFFFFull;
+    uint16_t pos[F::kMaxTok];  // token position - e (< kTile)
+    uint16_t lit[F::kMaxTok];  // saturated at kSat
+    uint16_t ml[F::kMaxTok];
+    uint32_t off[F::kMaxTok];
+    uint32_t out[F::kMaxTok];       // output offset - d0
+    uint32_t deps[kGroupTok];       // executing: per group token, its match's in-group source
+    CDB_HD uint32_t& dep(uint32_t i, uint32_t g0) { return deps[i - g0]; }
+};
+
+// ---------------------------------------------------------------------------
 // Shared memory of one CTA.
 template <class F>
 struct Shm {
@@ -464,13 +494,7 @@ struct Shm {
             uint32_t cand_exit[kSupers][kCand];
             uint8_t ovr[kSupers][kSupSegs];       // exact-walk entries
         } p;
-        struct {
-            uint32_t pos[kMaxTok];  // token position - e
-            uint32_t lit[kMaxTok];  // saturated at 2^32 - 1
-            uint32_t ml[kMaxTok];
-            uint32_t off[kMaxTok];
-            uint32_t out[kMaxTok];  // output offset - d0
-        } t;
+        TokRecs<F> t;
     } u;
     alignas(16) uint8_t ring[kRing];
     uint32_t pend_bits[kGroupOut / 32 + 8];
@@ -920,9 +944,10 @@ struct Chunk {
                     ol = 0;
                     nx = next_of(in, b, lim, P, &ol);
                 }
+                constexpr uint64_t kSat = TokRecs<F>::kSat;
                 s.u.t.pos[i] = static_cast<uint32_t>(P - e);
-                s.u.t.lit[i] = sq.lit > 0xFFFFFFFFull ? 0xFFFFFFFFu : static_cast<uint32_t>(sq.lit);
-                s.u.t.ml[i] = sq.ml > 0xFFFFFFFFull ? 0xFFFFFFFFu : static_cast<uint32_t>(sq.ml);
+                s.u.t.lit[i] = static_cast<uint32_t>(sq.lit > kSat ? kSat : sq.lit);
+                s.u.t.ml[i] = static_cast<uint32_t>(sq.ml > kSat ? kSat : sq.ml);
                 s.u.t.off[i] = sq.off;
                 s.u.t.out[i] = static_cast<uint32_t>(o);
                 // the first failing or terminal token ends the chunk; a step
@@ -1042,9 +1067,9 @@ struct Chunk {
     }
 
     // Token i's match if its source is ready: copied, then published.
-    CDB_HD bool try_match(const Ring& rg, uint32_t i, uint64_t G0) {
+    CDB_HD bool try_match(const Ring& rg, uint32_t i, uint32_t g0, uint64_t G0) {
         // the in-group part of its source, packed at the literal phase
-        const uint32_t dep = s.u.t.pos[i];
+        const uint32_t dep = s.u.t.dep(i, g0);
         const uint32_t lo = dep & 0xFFFFu, hi = dep >> 16;
         if (lo < hi && !bits_clear(lo, hi)) return false;
         const uint32_t lit = s.u.t.lit[i], ml = s.u.t.ml[i], off = s.u.t.off[i];
@@ -1112,9 +1137,9 @@ struct Chunk {
                     const uint64_t ms = o + lit, src = ms - s.u.t.off[i];
                     const uint64_t lo = src > G0 ? src : G0;
                     const uint64_t hi = src + ml < ms ? src + ml : ms;
-                    s.u.t.pos[i] = lo < hi ? static_cast<uint32_t>(lo - G0) |
-                                                 (static_cast<uint32_t>(hi - G0) << 16)
-                                           : 0u;
+                    s.u.t.dep(i, g0) = lo < hi ? static_cast<uint32_t>(lo - G0) |
+                                                     (static_cast<uint32_t>(hi - G0) << 16)
+                                               : 0u;
                 }
             }
             s.pend[t] = pm;
@@ -1135,7 +1160,7 @@ struct Chunk {
                 // warp's lanes then hold consecutive tokens and copy together
                 for (uint32_t k = 0; k < kPerThread; ++k)
                     if (pm & (1u << k)) {
-                        if (try_match(rg, g0 + t + k * kThreads, G0))
+                        if (try_match(rg, g0 + t + k * kThreads, g0, G0))
                             pm = static_cast<uint8_t>(pm & ~(1u << k));
                         break;
                     }
@@ -1156,7 +1181,7 @@ struct Chunk {
             for (uint32_t t = 0; t < kThreads; ++t) {
                 uint8_t pm = s.pend[t];
                 for (uint32_t k = 0; k < kPerThread; ++k)
-                    if ((pm & (1u << k)) && try_match(rg, g0 + t + k * kThreads, G0))
+                    if ((pm & (1u << k)) && try_match(rg, g0 + t + k * kThreads, g0, G0))
                         pm = static_cast<uint8_t>(pm & ~(1u << k));
                 s.pend[t] = pm;
                 any = any || pm != 0;
