@@ -147,11 +147,40 @@ namespace {
 // exactly bytes_written per chunk, bounded by the chunk's capacity (a longer
 // device-reported length is a device fault: the chunk is stamped CUDA and
 // the wave fails, as src/stream.cpp:163-184 does).
-// Every record is checked before any byte moves; the copies of a wave of
-// kParallelScatter bytes or more are split into chunk ranges of about equal
-// bytes over up to 16 host threads (the calling thread takes one range).
-constexpr size_t kParallelScatter = size_t{4} << 20;
+// Host copies of a wave: kParallelCopy bytes or more are split into ranges
+// of consecutive chunks of about equal bytes over up to 16 host threads (the
+// calling thread takes the first range); fewer go on the calling thread.
+// bytes(j) is chunk j's share; copy(j0, j1, k) copies chunks [j0, j1), k
+// being the range's index (its starting offsets are the caller's to keep).
+constexpr size_t kParallelCopy = size_t{4} << 20;
 
+template <class Bytes, class Copy>
+void parallel_copy(size_t wn, size_t total, Bytes bytes, Copy copy) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const size_t nt = std::min<size_t>({hw ? hw : 1u, 16u, wn});
+    if (total < kParallelCopy || nt < 2) {
+        copy(size_t{0}, wn);
+        return;
+    }
+    std::vector<size_t> jb(1, 0);
+    size_t acc = 0;
+    for (size_t j = 0; j < wn; ++j) {
+        acc += bytes(j);
+        if (jb.size() < nt && acc >= total / nt * jb.size() && j + 1 < wn) jb.push_back(j + 1);
+    }
+    jb.push_back(wn);
+    std::vector<std::thread> threads;
+    size_t r = 1;
+    try {
+        for (; r + 1 < jb.size(); ++r) threads.emplace_back(copy, jb[r], jb[r + 1]);
+    } catch (...) {  // no thread to be had: the rest on this one
+        for (; r + 1 < jb.size(); ++r) copy(jb[r], jb[r + 1]);
+    }
+    copy(jb[0], jb[1]);
+    for (std::thread& th : threads) th.join();
+}
+
+// Every record is checked before any byte moves.
 cudec_status scatter_wave(cudec_chunk_result* wr, const unsigned char* staged,
                           void* const* dst, const size_t* caps, size_t begin, size_t wn) {
     size_t total = 0;
@@ -166,44 +195,18 @@ cudec_status scatter_wave(cudec_chunk_result* wr, const unsigned char* staged,
         }
         total += bw;
     }
-    // chunks [j0, j1) from staging offset off0
-    auto copy = [&](size_t j0, size_t j1, size_t off0) {
-        size_t off = off0;
-        for (size_t j = j0; j < j1; ++j) {
-            const size_t i = begin + j;
-            const size_t bw = static_cast<size_t>(wr[j].bytes_written);
-            if (bw != 0 && dst[i] != nullptr) std::memcpy(dst[i], staged + off, bw);
-            off += caps[i];
-        }
-    };
-    const unsigned hw = std::thread::hardware_concurrency();
-    const size_t nt = std::min<size_t>({hw ? hw : 1u, 16u, wn});
-    if (total < kParallelScatter || nt < 2) {
-        copy(0, wn, 0);
-        return CUDEC_OK;
-    }
-    // range boundaries at about total / nt decoded bytes each
-    std::vector<size_t> jb(1, 0), ob(1, 0);
-    size_t acc = 0, off = 0;
-    for (size_t j = 0; j < wn; ++j) {
-        acc += static_cast<size_t>(wr[j].bytes_written);
-        off += caps[begin + j];
-        if (jb.size() < nt && acc >= total / nt * jb.size() && j + 1 < wn) {
-            jb.push_back(j + 1);
-            ob.push_back(off);
-        }
-    }
-    jb.push_back(wn);
-    std::vector<std::thread> threads;
-    size_t r = 1;
-    try {
-        for (; r + 1 < jb.size(); ++r)
-            threads.emplace_back(copy, jb[r], jb[r + 1], ob[r]);
-    } catch (...) {  // no thread to be had: the rest on this one
-        for (; r + 1 < jb.size(); ++r) copy(jb[r], jb[r + 1], ob[r]);
-    }
-    copy(jb[0], jb[1], ob[0]);
-    for (std::thread& th : threads) th.join();
+    // staging offsets: chunk j's slot starts at the sum of the earlier caps
+    std::vector<size_t> at(wn + 1, 0);
+    for (size_t j = 0; j < wn; ++j) at[j + 1] = at[j] + caps[begin + j];
+    parallel_copy(
+        wn, total, [&](size_t j) { return static_cast<size_t>(wr[j].bytes_written); },
+        [&](size_t j0, size_t j1) {
+            for (size_t j = j0; j < j1; ++j) {
+                const size_t i = begin + j;
+                const size_t bw = static_cast<size_t>(wr[j].bytes_written);
+                if (bw != 0 && dst[i] != nullptr) std::memcpy(dst[i], staged + at[j], bw);
+            }
+        });
     return CUDEC_OK;
 }
 
@@ -297,7 +300,9 @@ cudec_status decode(cudec_stream_ctx& ctx, const void* const* src, const size_t*
         uint64_t* pm = static_cast<uint64_t*>(ctx.p_meta[b].p);
         // Sources laid out back to back (the usual packed batch) go up in one
         // copy straight from the caller's memory: a DMA when it is pinned, a
-        // driver-staged copy otherwise; no host staging pass either way.
+        // driver-staged copy otherwise (faster, measured, than packing them
+        // into the pinned staging on host threads first); scattered sources
+        // are packed into the staging.
         bool contiguous = !in_place;
         for (size_t j = 1; j < wn && contiguous; ++j) {
             const size_t i = begin + j;

@@ -344,6 +344,40 @@ def test_stream_host_output_one_buffer(cuda):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("packed", [True, False])
+def test_stream_pageable_sources_staged_by_threads(cuda, packed):
+    """Pageable source chunks of more than 4 MiB a wave, packed back to back
+    in one buffer or scattered: the call stages them on host threads; bytes
+    and records equal the oracle's."""
+    import torch
+    n = 400
+    raws = [raw_data(30000 + 101 * i, seed=1300 + i) for i in range(n)]
+    comps = [W.lz4_compress(r) for r in raws]
+    caps = [len(r) for r in raws]
+    if packed:
+        buf = np.frombuffer(b"".join(comps), dtype=np.uint8).copy()
+        offs = np.concatenate([[0], np.cumsum([len(c) for c in comps])[:-1]]).astype(np.uint64)
+        sp = (offs + np.uint64(buf.ctypes.data)).astype(np.uint64)
+    else:
+        srcs = [np.frombuffer(c, dtype=np.uint8).copy() for c in comps]
+        sp = np.array([x.ctypes.data for x in srcs], dtype=np.uint64)
+    assert sum(len(c) for c in comps) > (4 << 20)
+    sz = np.array([len(c) for c in comps], dtype=np.uint64)
+    cp = np.array(caps, dtype=np.uint64)
+    dsts = [torch.full((c,), 0xA5, dtype=torch.uint8, device=cuda) for c in caps]
+    dp = np.array([x.data_ptr() for x in dsts], dtype=np.uint64)
+    res = np.zeros(n, dtype=[("status", "<i4"), ("reserved", "<u4"), ("bytes_written", "<u8")])
+    ctx = cd.StreamContext()
+    st = ctx.decode(sp.ctypes.data, sz.ctypes.data, dp.ctypes.data, cp.ctypes.data, n,
+                    cd.MEM_DEVICE, res.ctypes.data)
+    ctx.close()
+    assert st == 0
+    for i in range(n):
+        assert int(res[i]["status"]) == 0 and int(res[i]["bytes_written"]) == caps[i]
+        assert dsts[i].cpu().numpy().tobytes() == raws[i], i
+
+
+@pytest.mark.gpu
 def test_stream_poison_latch_on_allocation_failure(cuda):
     """An impossible host-output staging size makes the grow allocation fail
     on the host side: CUDA status, every record defined, context poisoned,
