@@ -81,7 +81,7 @@ __device__ inline uint64_t xxh64_dev(const uint8_t* p, uint64_t n) {
 // two aligned block loads and a funnel shift (lzw::ld16_output), never a load
 // of a block that holds no requested byte.
 
-constexpr uint64_t kLaneCopyMax = 64;  // longer runs are copied by the whole warp
+constexpr uint64_t kLaneCopyMax = 128;  // longer runs are copied by the whole warp
 
 // The whole warp copies n bytes src -> dst (non-overlapping): destination-
 // aligned 16-byte stores, four in flight per lane.
